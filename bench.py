@@ -1,0 +1,394 @@
+"""Benchmark: Wilson-flow link-updates/s at 32^4, mixed (FP32 links, FP64 reductions)
+vs FP64, on B200.
+
+One "step" is one Luscher RK3 flow step (three fused stage kernels) over a whole
+32^4 configuration: 4 * 32^4 = 4,194,304 link-updates.  Inputs are seeded
+synthetic fields U = e^{i a H} (a = 0.35, H Gaussian traceless Hermitian per
+link), generated on the device; 32^4 links plus the generator field are larger
+than the 126 MB L2 (no flush needed).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32_12|fp32_18|fp64]
+  python bench.py --impl reference     # the reference's own CPU code on the host cores
+
+Multi-GPU (torchrun, one rank per GPU): every rank flows its own configuration
+(replicas; the flow of independent configurations has no data-path exchange),
+timing is the max over ranks, `value` the sum of all ranks' link-updates.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Wilson-flow link-updates/s at 32^4: mixed vs FP64 on GPU at dE/E<1e-6; %HBM"
+UNIT = "link-updates/s"
+DIMS = (32, 32, 32, 32)
+EPS = 0.01
+A = 0.35
+SEED = 20260
+T_CHECK = 400  # accuracy check: flow to t = 4.0 (config: eps 0.01, 400 steps)
+LINK_BYTES = {"fp64": 144, "fp32_18": 72, "fp32_12": 48}
+FORCE_BYTES = {"fp64": 64, "fp32_18": 32, "fp32_12": 32}
+
+
+def bytes_per_link_update(prec: str) -> int:
+    """Compulsory HBM bytes of one link through the three fused stages with
+    ping-pong link buffers: read + write the link per stage (6 s_U) and the
+    8-real generator written in stage 0, read + written in stage 1, read in
+    stage 2 (4 s_Z)."""
+    return 6 * LINK_BYTES[prec] + 4 * FORCE_BYTES[prec]
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(prec: str, dims):
+    """DRAM bytes per stage launch from the committed ncu summary, or None."""
+    name = "rk_stage_%s_%s.md" % ("x".join(str(d) for d in dims), prec)
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in self.rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------------------------
+# distributed plumbing (torchrun); single GPU needs none
+# ----------------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self, n_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.torch = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            self.torch = torch
+            torch.cuda.set_device(self.local)
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+            self.dev = torch.device("cuda", self.local) if backend == "nccl" else torch.device("cpu")
+
+    def barrier(self):
+        if self.torch:
+            self.dist.barrier()
+            if self.dev.type == "cuda":
+                self.torch.cuda.synchronize()
+
+    def max(self, v: float) -> float:
+        if not self.torch:
+            return v
+        t = self.torch.tensor([v], dtype=self.torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.torch:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------------------------
+# CPU side: the reference's own code (oracle/_ref/ref_flow) on the host cores
+# ----------------------------------------------------------------------------------------------
+def write_reference_input(path: Path, dims, seed: int) -> None:
+    from oracle import ymoracle as yo
+
+    yo.write_bin(yo.gen_expiah(dims, A, seed), path)
+
+
+def host_processes(per_proc_gb: float) -> int:
+    cores = os.cpu_count() or 1
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    avail_gb = None
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                avail_gb = int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    n = cores
+    if avail_gb:
+        n = min(n, max(1, int(0.5 * avail_gb / per_proc_gb)))
+    return max(1, min(n, 64))
+
+
+def run_reference(dims, nproc: int, steps: int):
+    """nproc concurrent single-rank reference processes, each flowing its own copy of
+    the seeded configuration `steps` RK3 steps.  Returns (link-updates/s, detail)."""
+    from oracle import ymoracle as yo
+
+    if not yo.ref_available():
+        return None, "oracle/_ref/ref_flow is not built"
+    with tempfile.TemporaryDirectory() as d:
+        conf = Path(d) / "conf.bin"
+        write_reference_input(conf, dims, SEED)
+        args = [str(yo.REF_BIN), "time", str(conf)] + [str(v) for v in dims] + [repr(EPS), str(steps)]
+        procs = [subprocess.Popen(args, stdout=subprocess.PIPE, text=True) for _ in range(nproc)]
+        outs = []
+        for p in procs:
+            out, _ = p.communicate()
+            if p.returncode != 0:
+                return None, "ref_flow failed"
+            outs.append(json.loads(out.strip().splitlines()[-1]))
+    t = max(o["flow_seconds"] for o in outs)
+    links = 4 * dims[0] * dims[1] * dims[2] * dims[3]
+    return nproc * links * steps / t, {"flow_seconds_max": t, "obs_seconds": outs[0]["obs_seconds"]}
+
+
+def reference_arm(args):
+    per_proc_gb = 3.6 * (DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]) / 32 ** 4
+    nproc = host_processes(per_proc_gb)
+    steps = 1
+    value, detail = run_reference(DIMS, nproc, steps)
+    if value is None:
+        print(json.dumps({"impl": "reference", "unavailable": detail}))
+        return
+    sample = ("%d concurrent single-rank reference processes (src/ compiled against a one-rank MPI "
+              "stand-in), each one RK3 step of its own 32^4 configuration" % nproc)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": 0, "ms_per_step": detail["flow_seconds_max"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded e^{iaH}, a=0.35)",
+        "config": {"workload": "32^4 Wilson flow, RK3 eps=0.01, reference CPU code", "lattice": list(DIMS),
+                   "parallelism": "%d host processes" % nproc},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------------------
+def our_arm(args, dist: Dist):
+    import ctypes
+
+    import numpy as np
+
+    from latticeyangmills_b200 import GluonField, _native as N
+
+    V = DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]
+    links = 4 * V
+    prec = args.precision
+    dev = dist.local
+    seed = SEED + 1000 * dist.rank
+
+    f = GluonField(DIMS, prec, device=dev)
+    f.init_links("expiah", A, seed)
+    f.time_steps(EPS, args.warmup)  # untimed warm-up
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.5)
+    f.time_steps(EPS, max(args.warmup, 3))  # brings clocks up before the sampled window
+    dist.barrier()
+    elapsed_ms, kernel_ms = f.time_steps(EPS, args.steps, kernels=False)
+    dist.barrier()
+    # stage-kernel durations, measured with events around every launch of a second timed pass
+    _, kernel_ms = f.time_steps(EPS, args.steps, kernels=True)
+    clocks.stop()
+    t_max = dist.max(elapsed_ms / 1e3)
+    value = dist.world * links * args.steps / t_max
+
+    # FP64 path on the same workload (the "vs FP64" of the metric)
+    fp64_value = None
+    if prec != "fp64":
+        g = GluonField(DIMS, "fp64", device=dev)
+        g.init_links("expiah", A, seed)
+        g.time_steps(EPS, args.warmup)
+        dist.barrier()
+        ms64, _ = g.time_steps(EPS, args.steps)
+        fp64_value = dist.world * links * args.steps / dist.max(ms64 / 1e3)
+        g.close()
+
+    # roofline of the dominant kernel (the fused RK stage)
+    peak, peak_kind = measured_peaks()
+    bpl = bytes_per_link_update(prec) * links / 3.0  # algorithmic bytes per stage launch
+    avg_launch_s = kernel_ms / 1e3 / (3 * args.steps)
+    achieved = bpl / avg_launch_s / 1e9
+    traffic = profiled_traffic(prec, DIMS)
+
+    # accuracy of the mixed form against FP64 at t = 4 (400 steps), same seeded field
+    accuracy = None
+    if not args.skip_accuracy and dist.rank == 0:
+        res = {}
+        for p in sorted({prec, "fp64"}):
+            h = GluonField(DIMS, p, device=dev)
+            h.init_links("expiah", A, SEED)
+            rows = h.flow(EPS, T_CHECK, 0, reunit_every=10 if p != "fp64" else 0)
+            res[p] = rows[-1]
+            h.close()
+        r64, rm = res["fp64"], res[prec]
+        accuracy = {"t": float(rm[1]), "t2E_fp64": float(r64[5]), "t2E": float(rm[5]),
+                    "rel_err_t2E": abs(float(rm[5]) - float(r64[5])) / abs(float(r64[5])),
+                    "Q_fp64": float(r64[3]), "abs_err_Q": abs(float(rm[3]) - float(r64[3])),
+                    "abs_err_plaq": abs(float(rm[2]) - float(r64[2])), "reunit_every": 10}
+
+    # end to end through the C ABI with host buffers: upload the .bin-layout FP64
+    # configuration from pinned memory, flow K steps, read the observables back
+    host = ctypes.c_void_p()
+    nbytes = links * 18 * 8
+    N.check(N.load().ymflow_host_alloc(nbytes, ctypes.byref(host)))
+    hbuf = np.ctypeslib.as_array(ctypes.cast(host, ctypes.POINTER(ctypes.c_double)), shape=(links * 18,))
+    hbuf[:] = f.download().reshape(-1)
+    e2e_iters = 3
+    f.upload(hbuf)
+    f.flow(EPS, 2, 0)  # warm path
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_iters):
+        f.upload(hbuf)
+        rows = f.flow(EPS, args.steps, 0, reunit_every=10 if prec != "fp64" else 0)
+    t_e2e = dist.max(time.perf_counter() - t0)
+    e2e_value = dist.world * links * args.steps * e2e_iters / t_e2e
+    N.load().ymflow_host_free(host)
+    rows_bytes = 2 * 48  # two measurement rows (before / after) come back per job
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.skip_cpu:
+        val, detail = run_reference(DIMS, 1, 1)
+        if val is not None:
+            cpu = {"value": val, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "one RK3 step of the 32^4 configuration by the reference's own code "
+                             "(oracle/_ref/ref_flow), one core"}
+    f.close()
+
+    if dist.rank == 0:
+        launches = 3 * args.steps
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if prec != "fp64" else "f64",
+            "data": "synthetic (seeded U = e^{iaH}, a = 0.35, generated on the device)",
+            "config": {"workload": "32^4 Wilson flow, Luscher RK3, eps = 0.01",
+                       "lattice": list(DIMS), "precision": prec,
+                       "reductions": "f64", "l2": "inputs larger than L2 (links + generator > 126 MB)",
+                       "parallelism": "replicas x%d" % dist.world,
+                       "fp64_link_updates_per_s": fp64_value,
+                       "mixed_over_fp64": (value / fp64_value) if fp64_value else None},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "rk_stage_kernel (fused RK3 stage)",
+                         "algorithmic_bytes_per_launch": bpl,
+                         "avg_launch_ms": avg_launch_s * 1e3},
+            "accuracy_vs_fp64": accuracy,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes / args.steps,
+                    "d2h_bytes_per_step": rows_bytes / args.steps,
+                    "what": "per job: ymflow_upload of the .bin-layout FP64 field from pinned host memory, "
+                            "ymflow_flow of K steps, observables rows back to the host"},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32_12", choices=["fp64", "fp32_18", "fp32_12"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-accuracy", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        # CPU-only: under torchrun rank 0 runs and prints, the other ranks exit at once
+        if int(os.environ.get("RANK", "0")) == 0:
+            reference_arm(args)
+        return
+    dist = Dist(args.gpus)
+    try:
+        our_arm(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,164 @@
+/*
+ * ymflow — C ABI of the B200 Wilson gradient-flow engine (libymflow.so).
+ *
+ * Drop-in for the hot path of the reference's FLOW application
+ * (GioPede/LatticeYangMills): the RK3 flow step, the Wilson force, the SU(3)
+ * exponential and the plaquette / clover energy / clover charge observables.
+ * Every entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Plain C types only; every call returns int status (0 = ok, < 0 = error)
+ *     except the constructors, which return a handle and write the status.
+ *   - Host buffers are caller-owned; device memory, streams and graphs belong
+ *     to the context.  One context per host thread: calls on one context are
+ *     not reentrant; separate contexts are independent (one CUDA stream each).
+ *   - Links on the host use the reference's .bin layout
+ *     (src/InputOutput/inputconf.cpp:114-155): site-major with x fastest,
+ *     site = x + Nx*(y + Ny*(z + Nz*t)), then mu = 0..3, then 18 doubles per
+ *     link, a row-major 3x3 complex matrix with (re, im) interleaved
+ *     (include/Math/su3.h:63).
+ *   - No call exits or aborts the process; the text of the last error is
+ *     available from ymflow_last_error().
+ */
+#ifndef YMFLOW_H
+#define YMFLOW_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define YMFLOW_API __attribute__((visibility("default")))
+#else
+#define YMFLOW_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define YMFLOW_OK 0
+#define YMFLOW_ERR_ARG (-1)         /* bad argument (null pointer, size, precision ...) */
+#define YMFLOW_ERR_CUDA (-2)        /* a CUDA call failed; see ymflow_last_error */
+#define YMFLOW_ERR_OOM (-3)         /* device or pinned host allocation failed */
+#define YMFLOW_ERR_NONFINITE (-4)   /* a measured observable was NaN or infinite */
+#define YMFLOW_ERR_UNITARITY (-5)   /* mixed path: links drifted from SU(3) beyond the limit */
+#define YMFLOW_ERR_CAPACITY (-6)    /* caller's output array too small */
+#define YMFLOW_ERR_STATE (-7)       /* call out of order (e.g. flow before upload) */
+#define YMFLOW_ERR_NODEVICE (-8)    /* no CUDA device, or the device is not sm_100 */
+
+/* ---- precisions ------------------------------------------------------------------- */
+#define YMFLOW_FP64 0     /* FP64 links (18 reals), FP64 arithmetic: the parity path */
+#define YMFLOW_FP32_18 1  /* FP32 links (18 reals) and site arithmetic, FP64 reductions */
+#define YMFLOW_FP32_12 2  /* FP32 two-row links (12 reals, third row rebuilt), FP64 reductions */
+
+/* ---- seeded synthetic fields (ymflow_init_links) ------------------------------------ */
+#define YMFLOW_FIELD_COLD 0    /* every link the identity */
+#define YMFLOW_FIELD_EXPIAH 1  /* U = e^{i a H}, H traceless Hermitian, iid N(0,1) reals */
+
+typedef struct ymflow_ctx ymflow_ctx;
+
+/* One measurement: the reference's SuperObs public fields
+ * (include/Observables/observable.h:60) plus the flow time and t^2 <E>. */
+typedef struct {
+    int32_t step;   /* flow steps taken before this measurement */
+    int32_t pad;
+    double t;       /* flow time, accumulated as t += eps (src/Apps/wilsonflow.cpp:126) */
+    double plaq;    /* SuperObs::plaq   = sum Re tr P / (18 V)               (superobs.cpp:125) */
+    double topc;    /* SuperObs::topc   = -sum Re tr(G G~) / (256 pi^2)      (superobs.cpp:114-126) */
+    double energy;  /* SuperObs::energy = sum Re tr(G G), raw clover sum     (superobs.cpp:109) */
+    double t2E;     /* t^2 <E> = -t^2 energy / (64 V) */
+} ymflow_obs;
+
+/* Library version string. */
+YMFLOW_API const char* ymflow_version(void);
+
+/* Number of usable (sm_100) CUDA devices. */
+YMFLOW_API int ymflow_device_count(int* count);
+
+/* Create a flow context for a dims[0] x dims[1] x dims[2] x dims[3] periodic
+ * lattice (x, y, z, t) on `device`.  Replaces WilsonFlow::createLattice
+ * (src/Apps/wilsonflow.cpp:87-91), which allocates the GluonField and the
+ * force field, and PureGauge's scratch fields (src/Actions/puregauge.cpp:18-25). */
+YMFLOW_API ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* status);
+
+/* Release every device resource of the context.  NULL is accepted. */
+YMFLOW_API void ymflow_destroy(ymflow_ctx* ctx);
+
+/* Text of the last error on this context (never NULL).  With ctx == NULL:
+ * the last error of a failed ymflow_create. */
+YMFLOW_API const char* ymflow_last_error(const ymflow_ctx* ctx);
+
+/* Load links from a host buffer in .bin layout (4*V*18 doubles).
+ * Replaces LatticeIO::InputConf::readConf's fill of the GluonField
+ * (src/InputOutput/inputconf.cpp:114-155). */
+YMFLOW_API int ymflow_upload(ymflow_ctx* ctx, const double* links_aos);
+
+/* Store the current links to a host buffer in .bin layout (4*V*18 doubles).
+ * (The reference's writer is a no-op, src/InputOutput/outputconf.cpp:102.) */
+YMFLOW_API int ymflow_download(ymflow_ctx* ctx, double* links_aos);
+
+/* Fill the links with a seeded synthetic field on the device: kind COLD or
+ * EXPIAH (scale a); then, if haar_frac > 0, replace that fraction of links
+ * (seeded Bernoulli) by Haar-random SU(3).  Same recipe as the test fixtures. */
+YMFLOW_API int ymflow_init_links(ymflow_ctx* ctx, int kind, double a, uint64_t seed, uint32_t config, double haar_frac);
+
+/* Plaquette, clover energy and clover charge of the current links.
+ * Replaces SuperObs::compute (src/Observables/superobs.cpp:31-128) including
+ * its MPI_Allreduce (:24-28).  out->step / out->t are the context's counters. */
+YMFLOW_API int ymflow_observables(ymflow_ctx* ctx, ymflow_obs* out);
+
+/* Flow nsteps Luscher RK3 steps of size eps (WilsonFlow::flowStep,
+ * src/Apps/wilsonflow.cpp:141-172).  A measurement is taken before the first
+ * step (row 0, as src/Apps/wilsonflow.cpp:120-123), after every
+ * `measure_every`-th step and after the last step; measure_every <= 0 measures
+ * only before and after.  Mixed precisions reunitarise in FP64 every
+ * `reunit_every` steps (<= 0: never; the FP64 path ignores it, as the
+ * reference never reunitarises).  Rows go to out[0 .. *n_out-1]; out_cap must
+ * hold them all (YMFLOW_ERR_CAPACITY otherwise, before any work).  Returns
+ * YMFLOW_ERR_NONFINITE if a measurement is NaN/inf, YMFLOW_ERR_UNITARITY if a
+ * reunitarisation saw a row norm off by more than 1e-3. */
+YMFLOW_API int ymflow_flow(ymflow_ctx* ctx, double eps, int nsteps, int measure_every, int reunit_every, ymflow_obs* out,
+                int out_cap, int* n_out);
+
+/* The flow generator Z_mu(x) = (i/2)[U Omega - (U Omega)^+]_traceless of the
+ * current links for one direction mu, as V full 3x3 Hermitian matrices (18
+ * doubles each, site order).  Replaces PureGauge::computeDerivative(mu)
+ * (src/Actions/puregauge.cpp:62-79; staples :36-54). */
+YMFLOW_API int ymflow_derivative(ymflow_ctx* ctx, int mu, double* z_host);
+
+/* e^{iQ} of n Hermitian traceless 3x3 matrices (18 doubles each, only the
+ * diagonal entries 0 and 1 and the upper triangle are read) on `device`.
+ * Replaces exp(const SU3&) (src/Math/su3.cpp:96-183); where that returns NaN
+ * (Q = 0, or rounding past acos's domain on a degenerate spectrum) this
+ * returns the exponential. */
+YMFLOW_API int ymflow_su3_exp(const double* q_host, double* r_host, int64_t n, int device);
+
+/* Reset the context's step and flow-time counters (a new configuration). */
+YMFLOW_API int ymflow_reset_time(ymflow_ctx* ctx);
+
+/* Device-timed flow steps for benchmarking: runs nsteps RK3 steps (no
+ * measurements) between two CUDA events on the context's stream and writes the
+ * elapsed milliseconds.  kernel_ms (optional, may be NULL) receives the summed
+ * duration of the stage kernels alone, timed with events around each launch. */
+YMFLOW_API int ymflow_time_steps(ymflow_ctx* ctx, double eps, int nsteps, float* elapsed_ms, float* kernel_ms);
+
+/* Tuning knobs.  key YMFLOW_OPT_BLOCK: threads per block of the stage kernel
+ * (32..256, multiple of 32); YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a
+ * captured CUDA graph (default), 0 = plain launches. */
+#define YMFLOW_OPT_BLOCK 1
+#define YMFLOW_OPT_GRAPH 2
+#define YMFLOW_OPT_OBS_BLOCK 3
+YMFLOW_API int ymflow_set_option(ymflow_ctx* ctx, int key, int64_t value);
+YMFLOW_API int ymflow_get_option(const ymflow_ctx* ctx, int key, int64_t* value);
+
+/* Page-locked host memory for transfers at full PCIe rate (cudaMallocHost). */
+YMFLOW_API int ymflow_host_alloc(int64_t bytes, void** ptr);
+YMFLOW_API int ymflow_host_free(void* ptr);
+
+/* Device bytes held by the context (links x2, force, staging, scratch). */
+YMFLOW_API int ymflow_device_bytes(const ymflow_ctx* ctx, int64_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* YMFLOW_H */

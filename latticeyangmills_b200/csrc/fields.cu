@@ -1,0 +1,271 @@
+// K3-K5: layout conversion, seeded field generation and FP64 reunitarisation.
+#include "expsu3.cuh"
+#include "kernels.h"
+
+namespace ym {
+
+// ---------------------------------------------------------------------------
+// K4: the reference's .bin layout (site-major, mu = 0..3, 18 doubles; see
+// src/InputOutput/inputconf.cpp:114-155) <-> the device SoA layout.
+// One thread per link; the AoS side is read/written 16 bytes at a time.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void pack_kernel(const double* __restrict__ aos, F u, int64_t V) {
+    const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (l >= 4 * V) return;
+    const int64_t s = l >> 2;
+    const int mu = int(l & 3);
+    const double2* src = reinterpret_cast<const double2*>(aos + l * 18);
+    M3<typename F::Real> a;
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+        const double2 v = src[e];
+        a.e[e / 3][e % 3] = cx(typename F::Real(v.x), typename F::Real(v.y));
+    }
+    u.store(mu, s, a);
+}
+
+template <class F>
+__global__ void unpack_kernel(F u, double* __restrict__ aos, int64_t V) {
+    const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (l >= 4 * V) return;
+    const int64_t s = l >> 2;
+    const int mu = int(l & 3);
+    const M3<typename F::Real> a = u.load(mu, s);
+    double2* dst = reinterpret_cast<double2*>(aos + l * 18);
+#pragma unroll
+    for (int e = 0; e < 9; e++) dst[e] = make_double2(double(a.e[e / 3][e % 3].re), double(a.e[e / 3][e % 3].im));
+}
+
+cudaError_t launch_pack(int prec, const double* aos, void* u, const Geo& g, cudaStream_t st) {
+    const int b = 256;
+    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
+    switch (prec) {
+        case kFP64: pack_kernel<<<nb, b, 0, st>>>(aos, FieldD18{(double2*)u, g.V}, g.V); break;
+        case kFP32_18: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF18{(float2*)u, g.V}, g.V); break;
+        case kFP32_12: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF12{(float2*)u, g.V}, g.V); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(int prec, const void* u, double* aos, const Geo& g, cudaStream_t st) {
+    const int b = 256;
+    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
+    switch (prec) {
+        case kFP64: unpack_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, aos, g.V); break;
+        case kFP32_18: unpack_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, aos, g.V); break;
+        case kFP32_12: unpack_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, aos, g.V); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// K5: seeded fields.  Philox4x32-10 (Salmon et al., SC'11) keyed by the 64-bit
+// seed, counter = (global link index in .bin order, config id, stream<<16 | block);
+// two 53-bit uniforms per output, Box-Muller for normals.  The CPU generator of
+// the test fixtures follows the same recipe; the two agree to the last few ulp
+// (libm vs CUDA transcendental rounding).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+    return (double(a >> 5) * 67108864.0 + double(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+enum { kStreamH = 0, kStreamHaar = 1, kStreamPick = 2 };
+
+__device__ __forceinline__ double2 gauss2(uint64_t seed, uint32_t config, uint64_t lidx, uint32_t stream,
+                                          uint32_t block) {
+    const uint4 o = philox4x32(make_uint4(uint32_t(lidx), uint32_t(lidx >> 32), config, (stream << 16) | block),
+                               make_uint2(uint32_t(seed), uint32_t(seed >> 32)));
+    const double u1 = 1.0 - u53(o.x, o.y);
+    const double u2 = u53(o.z, o.w);
+    const double r = sqrt(-2.0 * log(u1));
+    double sp, cp;
+    sincos(6.283185307179586 * u2, &sp, &cp);
+    return make_double2(r * cp, r * sp);
+}
+
+template <class F>
+__global__ void init_kernel(F u, int64_t V, int kind, double a, uint64_t seed, uint32_t config) {
+    const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (l >= 4 * V) return;
+    const int64_t s = l >> 2;
+    const int mu = int(l & 3);
+    using R = typename F::Real;
+    M3<double> m;
+    if (kind == kCold) {
+        mzero(m);
+        m.e[0][0].re = m.e[1][1].re = m.e[2][2].re = 1.0;
+    } else {
+        double g[10];
+#pragma unroll
+        for (int b = 0; b < 5; b++) {
+            const double2 v = gauss2(seed, config, uint64_t(l), kStreamH, b);
+            g[2 * b] = v.x;
+            g[2 * b + 1] = v.y;
+        }
+        const double tr = (g[0] + g[1] + g[2]) / 3.0;
+        Herm8<double> q;
+        q.d0 = a * (g[0] - tr);
+        q.d1 = a * (g[1] - tr);
+        q.z01 = cx(a * g[3], a * g[4]);
+        q.z02 = cx(a * g[5], a * g[6]);
+        q.z12 = cx(a * g[7], a * g[8]);
+        exp_iq(q, m);
+    }
+    M3<R> r;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) r.e[i][j] = cx(R(m.e[i][j].re), R(m.e[i][j].im));
+    u.store(mu, s, r);
+}
+
+// Rows 0 and 1 orthonormalised (Gram-Schmidt, FP64), row 2 = conj(row0 x row1).
+__device__ __forceinline__ void gram_schmidt(M3<double>& m) {
+    double n0 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) n0 += m.e[0][k].re * m.e[0][k].re + m.e[0][k].im * m.e[0][k].im;
+    n0 = rsqrt(n0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        m.e[0][k].re *= n0;
+        m.e[0][k].im *= n0;
+    }
+    double pr = 0.0, pi = 0.0;  // <row0, row1>
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        pr += m.e[0][k].re * m.e[1][k].re + m.e[0][k].im * m.e[1][k].im;
+        pi += m.e[0][k].re * m.e[1][k].im - m.e[0][k].im * m.e[1][k].re;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        m.e[1][k].re -= pr * m.e[0][k].re - pi * m.e[0][k].im;
+        m.e[1][k].im -= pr * m.e[0][k].im + pi * m.e[0][k].re;
+    }
+    double n1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) n1 += m.e[1][k].re * m.e[1][k].re + m.e[1][k].im * m.e[1][k].im;
+    n1 = rsqrt(n1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        m.e[1][k].re *= n1;
+        m.e[1][k].im *= n1;
+    }
+    reconstruct_row2(m);
+}
+
+template <class F>
+__global__ void haar_kernel(F u, int64_t V, double frac, uint64_t seed, uint32_t config) {
+    const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (l >= 4 * V) return;
+    const uint4 o = philox4x32(make_uint4(uint32_t(l), uint32_t(uint64_t(l) >> 32), config, uint32_t(kStreamPick) << 16),
+                               make_uint2(uint32_t(seed), uint32_t(seed >> 32)));
+    if (!(u53(o.x, o.y) < frac)) return;
+    M3<double> m;
+#pragma unroll
+    for (int b = 0; b < 9; b++) {
+        const double2 v = gauss2(seed, config, uint64_t(l), kStreamHaar, b);
+        m.e[b / 3][b % 3] = cx(v.x, v.y);
+    }
+    gram_schmidt(m);
+    using R = typename F::Real;
+    M3<R> r;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) r.e[i][j] = cx(R(m.e[i][j].re), R(m.e[i][j].im));
+    u.store(int(l & 3), l >> 2, r);
+}
+
+cudaError_t launch_init_links(int prec, void* u, const Geo& g, int kind, double a, uint64_t seed, uint32_t config,
+                              cudaStream_t st) {
+    const int b = 128;
+    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
+    switch (prec) {
+        case kFP64: init_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, g.V, kind, a, seed, config); break;
+        case kFP32_18: init_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, g.V, kind, a, seed, config); break;
+        case kFP32_12: init_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, g.V, kind, a, seed, config); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_haar_mix(int prec, void* u, const Geo& g, double frac, uint64_t seed, uint32_t config,
+                            cudaStream_t st) {
+    const int b = 128;
+    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
+    switch (prec) {
+        case kFP64: haar_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, g.V, frac, seed, config); break;
+        case kFP32_18: haar_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, g.V, frac, seed, config); break;
+        case kFP32_12: haar_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, g.V, frac, seed, config); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// K3: FP64 reunitarisation (mixed path only; the FP64 path never reunitarises,
+// as the reference never does).
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void reunit_kernel(F u, int64_t V, unsigned long long* deviation) {
+    const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    double dev = 0.0;
+    if (l < 4 * V) {
+        const int64_t s = l >> 2;
+        const int mu = int(l & 3);
+        const M3<typename F::Real> a = u.load(mu, s);
+        M3<double> m;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) m.e[i][j] = cx(double(a.e[i][j].re), double(a.e[i][j].im));
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            double n = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) n += m.e[i][k].re * m.e[i][k].re + m.e[i][k].im * m.e[i][k].im;
+            dev = fmax(dev, fabs(n - 1.0));
+        }
+        gram_schmidt(m);
+        using R = typename F::Real;
+        M3<R> r;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) r.e[i][j] = cx(R(m.e[i][j].re), R(m.e[i][j].im));
+        u.store(mu, s, r);
+    }
+    // warp max, then one atomic per warp (non-negative doubles order like their bit patterns)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dev = fmax(dev, __shfl_down_sync(0xffffffffu, dev, o));
+    if ((threadIdx.x & 31) == 0 && deviation) atomicMax(deviation, (unsigned long long)__double_as_longlong(dev));
+}
+
+cudaError_t launch_reunitarize(int prec, void* u, const Geo& g, unsigned long long* deviation, cudaStream_t st) {
+    const int b = 256;
+    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
+    switch (prec) {
+        case kFP64: reunit_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, g.V, deviation); break;
+        case kFP32_18: reunit_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, g.V, deviation); break;
+        case kFP32_12: reunit_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, g.V, deviation); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace ym

@@ -1,0 +1,53 @@
+// Host-side launchers of the device kernels (one translation unit per kernel
+// family).  All take a CUDA stream and return the launch's cudaError_t.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "field.cuh"
+
+namespace ym {
+
+enum Precision { kFP64 = 0, kFP32_18 = 1, kFP32_12 = 2 };
+
+// bytes of one stored link / one stored generator for a precision
+inline int link_elems(int prec) { return prec == kFP32_12 ? 6 : 9; }
+inline size_t link_bytes(int prec) { return prec == kFP64 ? 9 * 16 : size_t(link_elems(prec)) * 8; }
+inline size_t force_bytes(int prec) { return prec == kFP64 ? 64 : 32; }
+
+// One RK3 stage (0, 1, 2) over every link: staples, generator, RK combination
+// with the stored generator, e^{i eps_stage Z} and the link update uin -> uout.
+cudaError_t launch_rk_stage(int prec, int stage, const void* uin, void* uout, void* z, const Geo& g, double eps,
+                            int block, cudaStream_t st);
+
+// D_mu (18 doubles per site, site order) for one direction: the reference's
+// PureGauge::computeDerivative(mu).
+cudaError_t launch_force(int prec, int mu, const void* u, const Geo& g, double* out, cudaStream_t st);
+// e^{iQ} for n Hermitian traceless matrices (18 doubles each).
+cudaError_t launch_exp(const double* q, double* r, int64_t n, cudaStream_t st);
+
+// Observables: per-block FP64 partial sums (plaq, energy, topc) into partials[3*nblocks],
+// then one block folds them in a fixed order into out[3] = (plaq, topc, energy) with the
+// reference's normalisations, out[3] = 1.0 when any value is not finite.
+int obs_blocks(const Geo& g, int block);
+cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* partials, int block,
+                               cudaStream_t st);
+cudaError_t launch_obs_finalize(const double* partials, int nblocks, const Geo& g, double* out, cudaStream_t st);
+
+// .bin layout (site-major, mu, 18 doubles) <-> device layout
+cudaError_t launch_pack(int prec, const double* aos, void* u, const Geo& g, cudaStream_t st);
+cudaError_t launch_unpack(int prec, const void* u, double* aos, const Geo& g, cudaStream_t st);
+
+// Seeded fields written straight into the device layout.
+enum FieldKind { kCold = 0, kExpIAH = 1 };
+cudaError_t launch_init_links(int prec, void* u, const Geo& g, int kind, double a, uint64_t seed, uint32_t config,
+                              cudaStream_t st);
+cudaError_t launch_haar_mix(int prec, void* u, const Geo& g, double frac, uint64_t seed, uint32_t config,
+                            cudaStream_t st);
+
+// FP64 Gram-Schmidt reunitarisation of every link; deviation[0] receives the
+// largest |row norm - 1| seen before the fix (as an ordered-int atomic max).
+cudaError_t launch_reunitarize(int prec, void* u, const Geo& g, unsigned long long* deviation, cudaStream_t st);
+
+}  // namespace ym

@@ -1,0 +1,179 @@
+// SU(3) algebra on the device, templated on the arithmetic type (double for the
+// FP64 path, float for the mixed path).
+//
+// A link is a 3x3 complex matrix, row-major, the same element order as the
+// reference's SU3 (include/Math/su3.h:63: 18 doubles, (re, im) interleaved).
+// Products are written out with fused multiply-adds; the reference evaluates
+// the same sums without FMA (su3.h:143-183), so the two agree to rounding.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ym {
+
+template <class R>
+struct Cx {
+    R re, im;
+};
+
+template <class R>
+struct M3 {
+    Cx<R> e[3][3];
+};
+
+// Hermitian traceless generator stored as 8 reals:
+//   d0 = Z00, d1 = Z11 (Z22 = -d0 - d1, real diagonal),
+//   z01, z02, z12 the upper off-diagonal entries (lower = conjugate).
+template <class R>
+struct Herm8 {
+    R d0, d1;
+    Cx<R> z01, z02, z12;
+};
+
+template <class R>
+__device__ __forceinline__ Cx<R> cx(R re, R im) {
+    Cx<R> c;
+    c.re = re;
+    c.im = im;
+    return c;
+}
+
+// c = op(a) * op(b) with op = identity or dagger (DA / DB).
+template <bool DA, bool DB, class R>
+__device__ __forceinline__ void mmul(const M3<R>& a, const M3<R>& b, M3<R>& c) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            R re = R(0), im = R(0);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const R xr = DA ? a.e[k][i].re : a.e[i][k].re;
+                const R xi = DA ? -a.e[k][i].im : a.e[i][k].im;
+                const R yr = DB ? b.e[j][k].re : b.e[k][j].re;
+                const R yi = DB ? -b.e[j][k].im : b.e[k][j].im;
+                re = fma(xr, yr, re);
+                re = fma(-xi, yi, re);
+                im = fma(xr, yi, im);
+                im = fma(xi, yr, im);
+            }
+            c.e[i][j] = cx(re, im);
+        }
+    }
+}
+
+// c += op(a) * op(b)
+template <bool DA, bool DB, class R>
+__device__ __forceinline__ void mmul_acc(const M3<R>& a, const M3<R>& b, M3<R>& c) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            R re = c.e[i][j].re, im = c.e[i][j].im;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const R xr = DA ? a.e[k][i].re : a.e[i][k].re;
+                const R xi = DA ? -a.e[k][i].im : a.e[i][k].im;
+                const R yr = DB ? b.e[j][k].re : b.e[k][j].re;
+                const R yi = DB ? -b.e[j][k].im : b.e[k][j].im;
+                re = fma(xr, yr, re);
+                re = fma(-xi, yi, re);
+                im = fma(xr, yi, im);
+                im = fma(xi, yr, im);
+            }
+            c.e[i][j] = cx(re, im);
+        }
+    }
+}
+
+template <class R>
+__device__ __forceinline__ void mzero(M3<R>& a) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) a.e[i][j] = cx(R(0), R(0));
+}
+
+template <class R>
+__device__ __forceinline__ void madd(M3<R>& a, const M3<R>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            a.e[i][j].re += b.e[i][j].re;
+            a.e[i][j].im += b.e[i][j].im;
+        }
+}
+
+template <class R>
+__device__ __forceinline__ R re_trace(const M3<R>& a) {
+    return a.e[0][0].re + a.e[1][1].re + a.e[2][2].re;
+}
+
+// Re tr(a * b) and Re tr(a * b^+) without forming the product.
+template <class R>
+__device__ __forceinline__ R re_trace_mul(const M3<R>& a, const M3<R>& b) {
+    R s = R(0);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            s = fma(a.e[i][k].re, b.e[k][i].re, s);
+            s = fma(-a.e[i][k].im, b.e[k][i].im, s);
+        }
+    return s;
+}
+
+// Row 2 of an SU(3) matrix from rows 0 and 1: r2 = conj(r0 x r1).
+template <class R>
+__device__ __forceinline__ void reconstruct_row2(M3<R>& a) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int i = (k + 1) % 3, j = (k + 2) % 3;
+        const Cx<R> p = a.e[0][i], q = a.e[1][j], r = a.e[0][j], s = a.e[1][i];
+        R re = p.re * q.re - p.im * q.im - (r.re * s.re - r.im * s.im);
+        R im = p.re * q.im + p.im * q.re - (r.re * s.im + r.im * s.re);
+        a.e[2][k] = cx(re, -im);
+    }
+}
+
+// Flow generator from X = U * Omega (Omega the staple sum):
+//   Z = (i/2) [X - X^+]_traceless   (Hermitian, traceless),
+// the quantity the reference returns from PureGauge::computeDerivative
+// (src/Actions/puregauge.cpp:62-79, where X is formed as (Omega^+ U^+)^+).
+template <class R>
+__device__ __forceinline__ Herm8<R> force_from_x(const M3<R>& x) {
+    Herm8<R> z;
+    const R i0 = x.e[0][0].im, i1 = x.e[1][1].im, i2 = x.e[2][2].im;
+    const R mean = (i0 + i1 + i2) * R(1.0 / 3.0);
+    z.d0 = mean - i0;
+    z.d1 = mean - i1;
+    // (i/2)(a + ib) = (-b/2, a/2) with a + ib = X_ij - conj(X_ji)
+    z.z01 = cx(R(-0.5) * (x.e[0][1].im + x.e[1][0].im), R(0.5) * (x.e[0][1].re - x.e[1][0].re));
+    z.z02 = cx(R(-0.5) * (x.e[0][2].im + x.e[2][0].im), R(0.5) * (x.e[0][2].re - x.e[2][0].re));
+    z.z12 = cx(R(-0.5) * (x.e[1][2].im + x.e[2][1].im), R(0.5) * (x.e[1][2].re - x.e[2][1].re));
+    return z;
+}
+
+template <class R>
+__device__ __forceinline__ Herm8<R> h8_axpby(R a, const Herm8<R>& x, R b, const Herm8<R>& y) {
+    Herm8<R> r;
+    r.d0 = a * x.d0 - b * y.d0;
+    r.d1 = a * x.d1 - b * y.d1;
+    r.z01 = cx(a * x.z01.re - b * y.z01.re, a * x.z01.im - b * y.z01.im);
+    r.z02 = cx(a * x.z02.re - b * y.z02.re, a * x.z02.im - b * y.z02.im);
+    r.z12 = cx(a * x.z12.re - b * y.z12.re, a * x.z12.im - b * y.z12.im);
+    return r;
+}
+
+template <class R>
+__device__ __forceinline__ Herm8<R> h8_scale(R a, const Herm8<R>& x) {
+    Herm8<R> r;
+    r.d0 = a * x.d0;
+    r.d1 = a * x.d1;
+    r.z01 = cx(a * x.z01.re, a * x.z01.im);
+    r.z02 = cx(a * x.z02.re, a * x.z02.im);
+    r.z12 = cx(a * x.z12.re, a * x.z12.im);
+    return r;
+}
+
+}  // namespace ym

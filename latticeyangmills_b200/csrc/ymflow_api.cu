@@ -1,0 +1,571 @@
+// C ABI of libymflow (declared in include/ymflow.h): the flow context, its
+// device buffers, the RK3 step sequence (optionally replayed as a CUDA graph)
+// and the measurement schedule of the reference's WilsonFlow::applyWilsonFlow
+// (src/Apps/wilsonflow.cpp:115-136).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "ymflow.h"
+
+using namespace ym;
+
+struct ymflow_ctx {
+    int dims[4] = {0, 0, 0, 0};
+    int prec = 0;
+    int device = 0;
+    Geo geo{};
+    cudaStream_t stream = nullptr;
+    void* u[2] = {nullptr, nullptr};  // ping-pong link buffers
+    int cur = 0;                      // which of u[] holds the current field
+    void* z = nullptr;                // RK generator, 8 reals per link
+    double* staging = nullptr;        // .bin-layout device buffer for upload/download
+    double* partials = nullptr;       // observables: 3 doubles per block
+    int partial_cap = 0;
+    double* meas = nullptr;           // measurement rows on the device, 4 doubles each
+    int meas_cap = 0;
+    double* meas_host = nullptr;      // pinned copy of the rows
+    unsigned long long* deviation = nullptr;  // reunitarisation drift (ordered bits)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    double graph_eps[2] = {0.0, 0.0};
+    int graph_block[2] = {0, 0};
+    std::vector<cudaEvent_t> events;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int block = 128;
+    int obs_block = 128;
+    bool use_graph = true;
+    bool loaded = false;
+    int64_t step = 0;
+    double t = 0.0;
+    int64_t bytes = 0;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+};
+
+int fail(ymflow_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(ymflow_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, e == cudaErrorMemoryAllocation ? YMFLOW_ERR_OOM : YMFLOW_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define YM_CK(ctx, call, what)                               \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+int64_t link_count(const ymflow_ctx* c) { return 4 * c->geo.V; }
+
+int dev_alloc(ymflow_ctx* c, void** p, size_t bytes, const char* what) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return cuda_fail(c, e, what);
+    }
+    c->bytes += int64_t(bytes);
+    return YMFLOW_OK;
+}
+
+int ensure_staging(ymflow_ctx* c) {
+    if (c->staging) return YMFLOW_OK;
+    return dev_alloc(c, (void**)&c->staging, size_t(link_count(c)) * 18 * sizeof(double), "staging buffer");
+}
+
+int ensure_partials(ymflow_ctx* c) {
+    const int nb = obs_blocks(c->geo, c->obs_block);
+    if (nb <= c->partial_cap) return YMFLOW_OK;
+    if (c->partials) {
+        cudaFree(c->partials);
+        c->bytes -= int64_t(c->partial_cap) * 3 * sizeof(double);
+        c->partials = nullptr;
+    }
+    int r = dev_alloc(c, (void**)&c->partials, size_t(nb) * 3 * sizeof(double), "observable partials");
+    if (r == YMFLOW_OK) c->partial_cap = nb;
+    return r;
+}
+
+int ensure_meas(ymflow_ctx* c, int rows) {
+    if (rows <= c->meas_cap) return YMFLOW_OK;
+    if (c->meas) {
+        cudaFree(c->meas);
+        c->bytes -= int64_t(c->meas_cap) * 4 * sizeof(double);
+        c->meas = nullptr;
+    }
+    if (c->meas_host) {
+        cudaFreeHost(c->meas_host);
+        c->meas_host = nullptr;
+    }
+    c->meas_cap = 0;
+    int r = dev_alloc(c, (void**)&c->meas, size_t(rows) * 4 * sizeof(double), "measurement rows");
+    if (r != YMFLOW_OK) return r;
+    cudaError_t e = cudaMallocHost((void**)&c->meas_host, size_t(rows) * 4 * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(c, e, "pinned measurement rows");
+    c->meas_cap = rows;
+    return YMFLOW_OK;
+}
+
+void drop_graphs(ymflow_ctx* c) {
+    for (int i = 0; i < 2; i++) {
+        if (c->graph[i]) cudaGraphExecDestroy(c->graph[i]);
+        c->graph[i] = nullptr;
+    }
+}
+
+// The three stage launches of one RK3 step starting from u[from].
+cudaError_t enqueue_step(ymflow_ctx* c, int from, double eps, cudaEvent_t* ev) {
+    void* a = c->u[from];
+    void* b = c->u[1 - from];
+    const void* in[3] = {a, b, a};
+    void* out[3] = {b, a, b};
+    for (int s = 0; s < 3; s++) {
+        if (ev) cudaEventRecord(ev[2 * s], c->stream);
+        cudaError_t e = launch_rk_stage(c->prec, s, in[s], out[s], c->z, c->geo, eps, c->block, c->stream);
+        if (e != cudaSuccess) return e;
+        if (ev) cudaEventRecord(ev[2 * s + 1], c->stream);
+    }
+    return cudaSuccess;
+}
+
+int run_step(ymflow_ctx* c, double eps, cudaEvent_t* ev) {
+    const int from = c->cur;
+    if (c->use_graph && !ev) {
+        if (!c->graph[from] || c->graph_eps[from] != eps || c->graph_block[from] != c->block) {
+            if (c->graph[from]) cudaGraphExecDestroy(c->graph[from]);
+            c->graph[from] = nullptr;
+            cudaGraph_t g = nullptr;
+            YM_CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin step capture");
+            cudaError_t le = enqueue_step(c, from, eps, nullptr);
+            cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
+            if (le != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return cuda_fail(c, le, "stage launch during capture");
+            }
+            YM_CK(c, ee, "end step capture");
+            cudaError_t ie = cudaGraphInstantiate(&c->graph[from], g, 0);
+            cudaGraphDestroy(g);
+            YM_CK(c, ie, "instantiate step graph");
+            c->graph_eps[from] = eps;
+            c->graph_block[from] = c->block;
+        }
+        YM_CK(c, cudaGraphLaunch(c->graph[from], c->stream), "launch step graph");
+    } else {
+        YM_CK(c, enqueue_step(c, from, eps, ev), "stage launch");
+    }
+    c->cur = 1 - from;
+    return YMFLOW_OK;
+}
+
+// Observables of the current field into meas row `row` (device).
+int enqueue_measure(ymflow_ctx* c, int row) {
+    int r = ensure_partials(c);
+    if (r != YMFLOW_OK) return r;
+    YM_CK(c, launch_observables(c->prec, c->u[c->cur], c->geo, c->partials, c->obs_block, c->stream),
+          "observables launch");
+    YM_CK(c, launch_obs_finalize(c->partials, obs_blocks(c->geo, c->obs_block), c->geo, c->meas + 4 * row, c->stream),
+          "observables fold");
+    return YMFLOW_OK;
+}
+
+void fill_obs(const ymflow_ctx* c, const double* m, int64_t step, double t, ymflow_obs* o) {
+    o->step = int32_t(step);
+    o->pad = 0;
+    o->t = t;
+    o->plaq = m[0];
+    o->topc = m[1];
+    o->energy = m[2];
+    o->t2E = -t * t * m[2] / (64.0 * double(c->geo.V));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ymflow_version(void) { return "ymflow 0.1 (sm_100a)"; }
+
+int ymflow_device_count(int* count) {
+    if (!count) return YMFLOW_ERR_ARG;
+    *count = 0;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return YMFLOW_OK;
+    }
+    int k = 0;
+    for (int d = 0; d < n; d++) {
+        int major = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) == cudaSuccess && major == 10) k++;
+    }
+    *count = k;
+    return YMFLOW_OK;
+}
+
+ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* status) {
+    auto set = [&](int s, const std::string& m) {
+        if (status) *status = s;
+        g_create_error = m;
+    };
+    if (!dims) {
+        set(YMFLOW_ERR_ARG, "dims is NULL");
+        return nullptr;
+    }
+    int64_t V = 1;
+    for (int i = 0; i < 4; i++) {
+        if (dims[i] < 1 || dims[i] > 4096) {
+            set(YMFLOW_ERR_ARG, "lattice extents must be in 1..4096");
+            return nullptr;
+        }
+        V *= dims[i];
+    }
+    if (V > (int64_t(1) << 31)) {
+        set(YMFLOW_ERR_ARG, "lattice volume above 2^31 sites");
+        return nullptr;
+    }
+    if (precision < YMFLOW_FP64 || precision > YMFLOW_FP32_12) {
+        set(YMFLOW_ERR_ARG, "unknown precision");
+        return nullptr;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        set(YMFLOW_ERR_NODEVICE, "no CUDA device with that index");
+        return nullptr;
+    }
+    int major = 0, minor = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
+    if (major != 10 || minor != 0) {
+        set(YMFLOW_ERR_NODEVICE, "libymflow is built for sm_100a (B200); device has sm_" + std::to_string(major) +
+                                     std::to_string(minor));
+        return nullptr;
+    }
+    ymflow_ctx* c = new (std::nothrow) ymflow_ctx();
+    if (!c) {
+        set(YMFLOW_ERR_OOM, "host allocation failed");
+        return nullptr;
+    }
+    DeviceGuard guard(device);
+    c->device = device;
+    c->prec = precision;
+    for (int i = 0; i < 4; i++) {
+        c->dims[i] = dims[i];
+        c->geo.n[i] = dims[i];
+    }
+    c->geo.stride[0] = 1;
+    c->geo.stride[1] = dims[0];
+    c->geo.stride[2] = int64_t(dims[0]) * dims[1];
+    c->geo.stride[3] = int64_t(dims[0]) * dims[1] * dims[2];
+    c->geo.V = V;
+    int r = YMFLOW_OK;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) r = YMFLOW_ERR_CUDA;
+    const size_t ub = size_t(4 * V) * link_bytes(precision);
+    const size_t zb = size_t(4 * V) * force_bytes(precision);
+    if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[0], ub, "link buffer 0");
+    if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[1], ub, "link buffer 1");
+    if (r == YMFLOW_OK) r = dev_alloc(c, &c->z, zb, "force buffer");
+    if (r == YMFLOW_OK) r = dev_alloc(c, (void**)&c->deviation, sizeof(unsigned long long), "drift flag");
+    if (r == YMFLOW_OK) r = ensure_partials(c);
+    if (r == YMFLOW_OK) r = ensure_meas(c, 16);
+    if (r == YMFLOW_OK && (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess))
+        r = YMFLOW_ERR_CUDA;
+    if (r != YMFLOW_OK) {
+        set(r, c->err.empty() ? "context setup failed" : c->err);
+        ymflow_destroy(c);
+        return nullptr;
+    }
+    if (status) *status = YMFLOW_OK;
+    return c;
+}
+
+void ymflow_destroy(ymflow_ctx* c) {
+    if (!c) return;
+    DeviceGuard guard(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    for (void* p : {c->u[0], c->u[1], c->z, (void*)c->staging, (void*)c->partials, (void*)c->meas,
+                    (void*)c->deviation})
+        if (p) cudaFree(p);
+    if (c->meas_host) cudaFreeHost(c->meas_host);
+    for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* ymflow_last_error(const ymflow_ctx* c) {
+    if (!c) return g_create_error.c_str();
+    return c->err.c_str();
+}
+
+int ymflow_upload(ymflow_ctx* c, const double* links) {
+    if (!c || !links) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_upload");
+    DeviceGuard guard(c->device);
+    int r = ensure_staging(c);
+    if (r != YMFLOW_OK) return r;
+    const size_t bytes = size_t(link_count(c)) * 18 * sizeof(double);
+    YM_CK(c, cudaMemcpyAsync(c->staging, links, bytes, cudaMemcpyHostToDevice, c->stream), "upload copy");
+    YM_CK(c, launch_pack(c->prec, c->staging, c->u[c->cur], c->geo, c->stream), "pack launch");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "upload");
+    c->loaded = true;
+    c->step = 0;
+    c->t = 0.0;
+    return YMFLOW_OK;
+}
+
+int ymflow_download(ymflow_ctx* c, double* links) {
+    if (!c || !links) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_download");
+    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    DeviceGuard guard(c->device);
+    int r = ensure_staging(c);
+    if (r != YMFLOW_OK) return r;
+    const size_t bytes = size_t(link_count(c)) * 18 * sizeof(double);
+    YM_CK(c, launch_unpack(c->prec, c->u[c->cur], c->staging, c->geo, c->stream), "unpack launch");
+    YM_CK(c, cudaMemcpyAsync(links, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream), "download copy");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "download");
+    return YMFLOW_OK;
+}
+
+int ymflow_init_links(ymflow_ctx* c, int kind, double a, uint64_t seed, uint32_t config, double haar_frac) {
+    if (!c) return YMFLOW_ERR_ARG;
+    if (kind != YMFLOW_FIELD_COLD && kind != YMFLOW_FIELD_EXPIAH) return fail(c, YMFLOW_ERR_ARG, "unknown field kind");
+    if (!(haar_frac >= 0.0 && haar_frac <= 1.0)) return fail(c, YMFLOW_ERR_ARG, "haar_frac outside [0, 1]");
+    DeviceGuard guard(c->device);
+    YM_CK(c, launch_init_links(c->prec, c->u[c->cur], c->geo, kind == YMFLOW_FIELD_COLD ? kCold : kExpIAH, a, seed,
+                               config, c->stream),
+          "init launch");
+    if (haar_frac > 0.0)
+        YM_CK(c, launch_haar_mix(c->prec, c->u[c->cur], c->geo, haar_frac, seed, config, c->stream), "haar launch");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "init links");
+    c->loaded = true;
+    c->step = 0;
+    c->t = 0.0;
+    return YMFLOW_OK;
+}
+
+int ymflow_observables(ymflow_ctx* c, ymflow_obs* out) {
+    if (!c || !out) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_observables");
+    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    DeviceGuard guard(c->device);
+    int r = enqueue_measure(c, 0);
+    if (r != YMFLOW_OK) return r;
+    YM_CK(c, cudaMemcpyAsync(c->meas_host, c->meas, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+          "observables copy");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "observables");
+    fill_obs(c, c->meas_host, c->step, c->t, out);
+    if (c->meas_host[3] != 0.0) return fail(c, YMFLOW_ERR_NONFINITE, "non-finite observable");
+    return YMFLOW_OK;
+}
+
+int ymflow_flow(ymflow_ctx* c, double eps, int nsteps, int measure_every, int reunit_every, ymflow_obs* out,
+                int out_cap, int* n_out) {
+    if (!c) return YMFLOW_ERR_ARG;
+    if (n_out) *n_out = 0;
+    if (nsteps < 0 || !std::isfinite(eps)) return fail(c, YMFLOW_ERR_ARG, "nsteps < 0 or eps not finite");
+    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    int rows = 1;
+    for (int s = 1; s <= nsteps; s++)
+        if ((measure_every > 0 && s % measure_every == 0) || s == nsteps) rows++;
+    if (out && out_cap < rows) return fail(c, YMFLOW_ERR_CAPACITY, "output holds " + std::to_string(out_cap) +
+                                                                       " rows, flow needs " + std::to_string(rows));
+    DeviceGuard guard(c->device);
+    int r = ensure_meas(c, rows);
+    if (r != YMFLOW_OK) return r;
+    std::vector<int64_t> row_step(rows);
+    std::vector<double> row_t(rows);
+    const bool reunit = c->prec != YMFLOW_FP64 && reunit_every > 0;
+    if (reunit) YM_CK(c, cudaMemsetAsync(c->deviation, 0, sizeof(unsigned long long), c->stream), "reset drift");
+    int row = 0;
+    if ((r = enqueue_measure(c, row)) != YMFLOW_OK) return r;
+    row_step[row] = c->step;
+    row_t[row] = c->t;
+    row++;
+    for (int s = 1; s <= nsteps; s++) {
+        if ((r = run_step(c, eps, nullptr)) != YMFLOW_OK) return r;
+        c->step++;
+        c->t += eps;
+        if (reunit && s % reunit_every == 0)
+            YM_CK(c, launch_reunitarize(c->prec, c->u[c->cur], c->geo, c->deviation, c->stream), "reunitarise");
+        if ((measure_every > 0 && s % measure_every == 0) || s == nsteps) {
+            if ((r = enqueue_measure(c, row)) != YMFLOW_OK) return r;
+            row_step[row] = c->step;
+            row_t[row] = c->t;
+            row++;
+        }
+    }
+    YM_CK(c, cudaMemcpyAsync(c->meas_host, c->meas, size_t(rows) * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                             c->stream),
+          "measurement copy");
+    unsigned long long dev_bits = 0;
+    if (reunit)
+        YM_CK(c, cudaMemcpyAsync(&dev_bits, c->deviation, sizeof(dev_bits), cudaMemcpyDeviceToHost, c->stream),
+              "drift copy");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "flow");
+    bool nonfinite = false;
+    for (int i = 0; i < rows; i++) {
+        if (out) fill_obs(c, c->meas_host + 4 * i, row_step[i], row_t[i], out + i);
+        if (c->meas_host[4 * i + 3] != 0.0) nonfinite = true;
+    }
+    if (n_out) *n_out = rows;
+    if (nonfinite) return fail(c, YMFLOW_ERR_NONFINITE, "non-finite observable during the flow");
+    if (reunit) {
+        double d;
+        std::memcpy(&d, &dev_bits, sizeof(d));
+        if (d > 1e-3) return fail(c, YMFLOW_ERR_UNITARITY, "links drifted from SU(3): |row norm - 1| = " +
+                                                                std::to_string(d));
+    }
+    return YMFLOW_OK;
+}
+
+int ymflow_derivative(ymflow_ctx* c, int mu, double* z_host) {
+    if (!c || !z_host || mu < 0 || mu > 3) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_derivative");
+    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    DeviceGuard guard(c->device);
+    int r = ensure_staging(c);
+    if (r != YMFLOW_OK) return r;
+    YM_CK(c, launch_force(c->prec, mu, c->u[c->cur], c->geo, c->staging, c->stream), "force launch");
+    YM_CK(c, cudaMemcpyAsync(z_host, c->staging, size_t(c->geo.V) * 18 * sizeof(double), cudaMemcpyDeviceToHost,
+                             c->stream),
+          "force copy");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "derivative");
+    return YMFLOW_OK;
+}
+
+int ymflow_su3_exp(const double* q_host, double* r_host, int64_t n, int device) {
+    if (!q_host || !r_host || n < 0) return YMFLOW_ERR_ARG;
+    if (n == 0) return YMFLOW_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return YMFLOW_ERR_NODEVICE;
+    }
+    DeviceGuard guard(device);
+    double* d = nullptr;
+    const size_t bytes = size_t(n) * 18 * sizeof(double);
+    if (cudaMalloc(&d, 2 * bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return YMFLOW_ERR_OOM;
+    }
+    cudaError_t e = cudaMemcpy(d, q_host, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_exp(d, d + size_t(n) * 18, n, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(r_host, d + size_t(n) * 18, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? YMFLOW_OK : YMFLOW_ERR_CUDA;
+}
+
+int ymflow_reset_time(ymflow_ctx* c) {
+    if (!c) return YMFLOW_ERR_ARG;
+    c->step = 0;
+    c->t = 0.0;
+    return YMFLOW_OK;
+}
+
+int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, float* kernel_ms) {
+    if (!c || !elapsed_ms || nsteps < 1) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_time_steps");
+    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    DeviceGuard guard(c->device);
+    const size_t nev = kernel_ms ? size_t(6) * nsteps : 0;
+    while (c->events.size() < nev) {
+        cudaEvent_t e;
+        YM_CK(c, cudaEventCreate(&e), "event create");
+        c->events.push_back(e);
+    }
+    YM_CK(c, cudaEventRecord(c->ev0, c->stream), "event record");
+    for (int s = 0; s < nsteps; s++) {
+        int r = run_step(c, eps, kernel_ms ? c->events.data() + 6 * s : nullptr);
+        if (r != YMFLOW_OK) return r;
+        c->step++;
+        c->t += eps;
+    }
+    YM_CK(c, cudaEventRecord(c->ev1, c->stream), "event record");
+    YM_CK(c, cudaEventSynchronize(c->ev1), "timed steps");
+    YM_CK(c, cudaEventElapsedTime(elapsed_ms, c->ev0, c->ev1), "elapsed time");
+    if (kernel_ms) {
+        double sum = 0.0;
+        for (int i = 0; i < 3 * nsteps; i++) {
+            float ms = 0.f;
+            YM_CK(c, cudaEventElapsedTime(&ms, c->events[2 * i], c->events[2 * i + 1]), "kernel time");
+            sum += ms;
+        }
+        *kernel_ms = float(sum);
+    }
+    return YMFLOW_OK;
+}
+
+int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
+    if (!c) return YMFLOW_ERR_ARG;
+    switch (key) {
+        case YMFLOW_OPT_BLOCK:
+            if (value < 32 || value > 256 || value % 32) return fail(c, YMFLOW_ERR_ARG, "block must be 32..256, /32");
+            c->block = int(value);
+            return YMFLOW_OK;
+        case YMFLOW_OPT_OBS_BLOCK:
+            if (value < 32 || value > 256 || value % 32) return fail(c, YMFLOW_ERR_ARG, "block must be 32..256, /32");
+            c->obs_block = int(value);
+            return YMFLOW_OK;
+        case YMFLOW_OPT_GRAPH:
+            c->use_graph = value != 0;
+            return YMFLOW_OK;
+        default: return fail(c, YMFLOW_ERR_ARG, "unknown option");
+    }
+}
+
+int ymflow_get_option(const ymflow_ctx* c, int key, int64_t* value) {
+    if (!c || !value) return YMFLOW_ERR_ARG;
+    switch (key) {
+        case YMFLOW_OPT_BLOCK: *value = c->block; return YMFLOW_OK;
+        case YMFLOW_OPT_OBS_BLOCK: *value = c->obs_block; return YMFLOW_OK;
+        case YMFLOW_OPT_GRAPH: *value = c->use_graph ? 1 : 0; return YMFLOW_OK;
+        default: return YMFLOW_ERR_ARG;
+    }
+}
+
+int ymflow_host_alloc(int64_t bytes, void** ptr) {
+    if (!ptr || bytes <= 0) return YMFLOW_ERR_ARG;
+    *ptr = nullptr;
+    cudaError_t e = cudaMallocHost(ptr, size_t(bytes));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        return e == cudaErrorMemoryAllocation ? YMFLOW_ERR_OOM : YMFLOW_ERR_CUDA;
+    }
+    return YMFLOW_OK;
+}
+
+int ymflow_host_free(void* ptr) {
+    if (!ptr) return YMFLOW_OK;
+    return cudaFreeHost(ptr) == cudaSuccess ? YMFLOW_OK : YMFLOW_ERR_CUDA;
+}
+
+int ymflow_device_bytes(const ymflow_ctx* c, int64_t* bytes) {
+    if (!c || !bytes) return YMFLOW_ERR_ARG;
+    *bytes = c->bytes;
+    return YMFLOW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,230 @@
+"""Host-side mirror of the reference's FLOW application interface over libymflow.
+
+Names follow the reference so code and tests read alike:
+
+  GluonField        device-resident Field<SU3,4> (include/Math/field.h:52-76)
+  SuperObs          plaq / energy / topc observable (include/Observables/superobs.h)
+  WilsonFlow        the FLOW app (include/Apps/wilsonflow.h): applyWilsonFlow,
+                    flowConfigurations, with the reference's step schedule
+  read_conf         LatticeIO::InputConf::readConf (src/InputOutput/inputconf.cpp:114-155)
+  get_input_list    InputConf::getInputList (inputconf.cpp:76-82)
+  write_flow_obs    LatticeIO::OutputObs::writeFlowObs (src/InputOutput/outputobs.cpp:64-84)
+
+Every computation runs in libymflow.so on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+from typing import Iterable, List, Sequence
+
+import numpy as np
+
+from . import _native as N
+
+
+def _dims(size: Sequence[int]):
+    if len(size) != 4:
+        raise ValueError("lattice size must have 4 extents (x, y, z, t)")
+    return N._I4(*[int(v) for v in size])
+
+
+def volume(size: Sequence[int]) -> int:
+    return int(size[0]) * int(size[1]) * int(size[2]) * int(size[3])
+
+
+def read_conf(path, size: Sequence[int]) -> np.ndarray:
+    """Links of a .bin configuration: raw native-endian doubles, per global site
+    (x fastest) 4 links of 18 doubles (inputconf.cpp:114-155).  Shape
+    (Nt, Nz, Ny, Nx, 4, 18)."""
+    n = volume(size) * 4 * 18
+    a = np.fromfile(str(path), dtype=np.float64)
+    if a.size != n:
+        raise ValueError(f"{path}: {a.size * 8} bytes, expected {n * 8} for lattice {tuple(size)}")
+    return a.reshape(size[3], size[2], size[1], size[0], 4, 18)
+
+
+def write_conf(path, links: np.ndarray) -> None:
+    """Writes links in the .bin layout read_conf reads (the reference's writer
+    is a no-op, src/InputOutput/outputconf.cpp:102)."""
+    np.ascontiguousarray(links, dtype=np.float64).tofile(str(path))
+
+
+def get_input_list(input_dir) -> List[str]:
+    """Every *.bin in input_dir, sorted by path (inputconf.cpp:76-82)."""
+    return sorted(str(p) for p in Path(input_dir).iterdir() if p.suffix == ".bin")
+
+
+def write_flow_obs(output_dir, conf_num: int, matrix: Iterable[Sequence[float]]) -> Path:
+    """OutputDir/flow/confNNNN.dat with the header and "%lf\\t" rows of
+    src/InputOutput/outputobs.cpp:64-84 (columns t, plaq, topc, energy)."""
+    d = Path(output_dir) / "flow"
+    d.mkdir(parents=True, exist_ok=True)
+    p = d / ("conf%04d.dat" % conf_num)
+    with open(p, "w") as f:
+        f.write("Flow Time\tPlaq.\tTopc.\tEnerg.\t\n")
+        for row in matrix:
+            f.write("".join("%f\t" % v for v in row) + "\n")
+    return p
+
+
+class GluonField:
+    """A gauge field resident on one B200, in one of the three storage forms
+    ("fp64", "fp32_18", "fp32_12")."""
+
+    def __init__(self, size: Sequence[int], precision: str = "fp64", device: int = 0):
+        self.size = tuple(int(v) for v in size)
+        self.precision = precision
+        prec = N.PRECISIONS[precision]
+        lib = N.load()
+        st = ctypes.c_int(0)
+        self._ctx = lib.ymflow_create(_dims(self.size), prec, int(device), ctypes.byref(st))
+        if not self._ctx:
+            raise N.YmflowError(st.value, lib.ymflow_last_error(None).decode(errors="replace"))
+        self.sites = volume(self.size)
+
+    # lifetime
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            N.load().ymflow_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def ctx(self):
+        if not self._ctx:
+            raise RuntimeError("GluonField is closed")
+        return self._ctx
+
+    def _check(self, status: int) -> None:
+        N.check(status, self.ctx)
+
+    # data movement
+    def upload(self, links: np.ndarray) -> None:
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        if a.size != self.sites * 72:
+            raise ValueError("links must hold 4*V*18 doubles")
+        self._check(N.load().ymflow_upload(self.ctx, a.ctypes.data))
+
+    def download(self) -> np.ndarray:
+        a = np.empty((self.size[3], self.size[2], self.size[1], self.size[0], 4, 18), dtype=np.float64)
+        self._check(N.load().ymflow_download(self.ctx, a.ctypes.data))
+        return a
+
+    def init_links(self, kind: str = "expiah", a: float = 0.35, seed: int = 1, config: int = 0,
+                   haar_frac: float = 0.0) -> None:
+        k = {"cold": N.FIELD_COLD, "expiah": N.FIELD_EXPIAH}[kind]
+        self._check(N.load().ymflow_init_links(self.ctx, k, float(a), int(seed), int(config), float(haar_frac)))
+
+    # compute
+    def observables(self) -> N.Obs:
+        o = N.Obs()
+        self._check(N.load().ymflow_observables(self.ctx, ctypes.byref(o)))
+        return o
+
+    def flow(self, eps: float, nsteps: int, measure_every: int = 1, reunit_every: int = 0) -> np.ndarray:
+        """nsteps RK3 steps; rows (step, t, plaq, topc, energy, t2E)."""
+        rows = 1 + sum(1 for s in range(1, nsteps + 1)
+                       if (measure_every > 0 and s % measure_every == 0) or s == nsteps)
+        out = (N.Obs * rows)()
+        n = ctypes.c_int(0)
+        self._check(N.load().ymflow_flow(self.ctx, float(eps), int(nsteps), int(measure_every), int(reunit_every),
+                                         out, rows, ctypes.byref(n)))
+        return np.array([out[i].as_tuple() for i in range(n.value)])
+
+    def derivative(self, mu: int) -> np.ndarray:
+        """Z_mu at every site, shape (V, 18): PureGauge::computeDerivative(mu)."""
+        z = np.empty((self.sites, 18), dtype=np.float64)
+        self._check(N.load().ymflow_derivative(self.ctx, int(mu), z.ctypes.data))
+        return z
+
+    def reset_time(self) -> None:
+        self._check(N.load().ymflow_reset_time(self.ctx))
+
+    def time_steps(self, eps: float, nsteps: int, kernels: bool = False):
+        """(elapsed_ms, kernel_ms or None) of nsteps device-timed RK3 steps."""
+        el = ctypes.c_float(0)
+        km = ctypes.c_float(0)
+        self._check(N.load().ymflow_time_steps(self.ctx, float(eps), int(nsteps), ctypes.byref(el),
+                                               ctypes.byref(km) if kernels else None))
+        return el.value, (km.value if kernels else None)
+
+    def set_option(self, key: int, value: int) -> None:
+        self._check(N.load().ymflow_set_option(self.ctx, int(key), int(value)))
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_int64(0)
+        self._check(N.load().ymflow_device_bytes(self.ctx, ctypes.byref(b)))
+        return b.value
+
+
+def su3_exp(q: np.ndarray, device: int = 0) -> np.ndarray:
+    """e^{iQ} of Hermitian traceless matrices (..., 18) on the GPU: exp(const SU3&)."""
+    a = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 18)
+    r = np.empty_like(a)
+    st = N.load().ymflow_su3_exp(a.ctypes.data, r.ctypes.data, a.shape[0], int(device))
+    if st != N.OK:
+        raise N.YmflowError(st, "ymflow_su3_exp failed")
+    return r
+
+
+class SuperObs:
+    """plaq, energy and topc of a field, as the reference's SuperObs
+    (src/Observables/superobs.cpp:31-128)."""
+
+    def __init__(self):
+        self.plaq = self.energy = self.topc = float("nan")
+        self._field = None
+
+    def initObservable(self, field: GluonField) -> None:
+        self._field = field
+
+    def compute(self) -> None:
+        o = self._field.observables()
+        self.plaq, self.energy, self.topc = o.plaq, o.energy, o.topc
+
+
+class WilsonFlow:
+    """The FLOW app (src/Apps/wilsonflow.cpp) over libymflow."""
+
+    def __init__(self, tauFinal: float, epsilon: float):
+        self.m_tauFinal = float(tauFinal)
+        self.m_epsilon = float(epsilon)
+        self.field: GluonField | None = None
+
+    def createLattice(self, size: Sequence[int], precision: str = "fp64", device: int = 0) -> None:
+        self.field = GluonField(size, precision, device)
+
+    def nrows(self) -> int:
+        """int(tauFinal/epsilon) rows: row 0 at t = 0, then one per flow step,
+        hence int(tauFinal/epsilon) - 1 steps (src/Apps/wilsonflow.cpp:117,124)."""
+        return int(self.m_tauFinal / self.m_epsilon)
+
+    def applyWilsonFlow(self) -> np.ndarray:
+        """Flows the loaded field; rows (t, plaq, topc, energy) as flowObsMatrix
+        (src/Apps/wilsonflow.cpp:115-136)."""
+        nsteps = max(self.nrows() - 1, 0)
+        self.field.reset_time()
+        rows = self.field.flow(self.m_epsilon, nsteps, measure_every=1)
+        return rows[: max(self.nrows(), 1), [1, 2, 3, 4]]
+
+    def flowConfigurations(self, input_dir, output_dir) -> List[Path]:
+        """Every sorted *.bin of input_dir: read, flow, write flow/confNNNN.dat
+        (src/Apps/wilsonflow.cpp:96-109)."""
+        written = []
+        for conf_num, path in enumerate(get_input_list(input_dir)):
+            self.field.upload(read_conf(path, self.field.size))
+            written.append(write_flow_obs(output_dir, conf_num, self.applyWilsonFlow()))
+        return written

@@ -1,0 +1,69 @@
+"""Error paths of the C ABI on the GPU: every failure is a status code and a
+message, none aborts or leaves the context unusable."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_flow_before_upload_is_a_state_error():
+    from latticeyangmills_b200 import GluonField, YmflowError
+    from latticeyangmills_b200 import _native as N
+
+    with GluonField((4, 4, 4, 4)) as f:
+        with pytest.raises(YmflowError) as e:
+            f.flow(0.01, 1, 1)
+        assert e.value.status == N.ERR_STATE
+
+
+def test_output_capacity_checked_before_work():
+    from latticeyangmills_b200 import GluonField
+    from latticeyangmills_b200 import _native as N
+
+    with GluonField((4, 4, 4, 4)) as f:
+        f.init_links("expiah", 0.3, 1)
+        out = (N.Obs * 2)()
+        n = ctypes.c_int(-1)
+        st = N.load().ymflow_flow(f.ctx, 0.01, 5, 1, 0, out, 2, ctypes.byref(n))
+        assert st == N.ERR_CAPACITY and n.value == 0
+        assert b"rows" in N.load().ymflow_last_error(f.ctx)
+        assert f.observables().step == 0  # nothing flowed
+
+
+def test_nan_link_is_reported_and_context_recovers():
+    from latticeyangmills_b200 import GluonField, YmflowError
+    from latticeyangmills_b200 import _native as N
+
+    n = (4, 4, 4, 4)
+    with GluonField(n) as f:
+        f.init_links("expiah", 0.3, 1)
+        U = f.download()
+        bad = U.copy()
+        bad[1, 2, 3, 0, 2, 5] = np.nan
+        f.upload(bad)
+        with pytest.raises(YmflowError) as e:
+            f.flow(0.01, 2, 1)
+        assert e.value.status == N.ERR_NONFINITE
+        f.upload(U)  # the same context keeps working
+        rows = f.flow(0.01, 2, 1)
+        assert np.isfinite(rows).all()
+
+
+def test_bad_options_rejected():
+    from latticeyangmills_b200 import GluonField, YmflowError
+    from latticeyangmills_b200 import _native as N
+
+    with GluonField((4, 4, 4, 4)) as f:
+        for key, val in [(N.OPT_BLOCK, 48), (N.OPT_BLOCK, 1024), (99, 1)]:
+            with pytest.raises(YmflowError):
+                f.set_option(key, val)
+
+
+def test_wrong_size_upload_rejected_on_host():
+    from latticeyangmills_b200 import GluonField
+
+    with GluonField((4, 4, 4, 4)) as f:
+        with pytest.raises(ValueError):
+            f.upload(np.zeros(10))

@@ -1,0 +1,44 @@
+"""Host-side logic of the FLOW mirror that needs no GPU: the reference's step
+schedule, the .bin reader and the flow/confNNNN.dat writer."""
+import numpy as np
+import pytest
+
+from latticeyangmills_b200 import WilsonFlow, get_input_list, read_conf, write_conf, write_flow_obs
+
+
+@pytest.mark.parametrize("tau,eps,rows", [(1.0, 0.01, 100), (4.0, 0.01, 400), (2.0, 0.01, 200),
+                                          (0.05, 0.01, 5), (6.0, 0.02, 300), (0.3, 0.1, 2)])
+def test_row_count_follows_reference(tau, eps, rows):
+    # int(tauFinal/epsilon) rows, row 0 at t = 0 (src/Apps/wilsonflow.cpp:117)
+    assert WilsonFlow(tau, eps).nrows() == rows == int(tau / eps)
+
+
+def test_flow_file_format(tmp_path):
+    m = [[0.0, 0.5, -0.25, -123.456789], [0.01, 0.6, 1e-7, -1.0]]
+    p = write_flow_obs(tmp_path, 3, m)
+    assert p.name == "conf0003.dat" and p.parent.name == "flow"
+    text = p.read_text()
+    # header and "%lf\t" cells of src/InputOutput/outputobs.cpp:66-81
+    assert text == ("Flow Time\tPlaq.\tTopc.\tEnerg.\t\n"
+                    "0.000000\t0.500000\t-0.250000\t-123.456789\t\n"
+                    "0.010000\t0.600000\t0.000000\t-1.000000\t\n")
+
+
+def test_read_conf_layout_and_size_check(tmp_path):
+    n = (2, 3, 4, 5)
+    a = np.arange(np.prod(n) * 72, dtype=np.float64)
+    write_conf(tmp_path / "c.bin", a)
+    U = read_conf(tmp_path / "c.bin", n)
+    assert U.shape == (5, 4, 3, 2, 4, 18)
+    # element k of link mu at (x,y,z,t) sits at ((site*4 + mu)*18 + k)
+    x, y, z, t, mu, k = 1, 2, 3, 4, 2, 7
+    site = x + 2 * (y + 3 * (z + 4 * t))
+    assert U[t, z, y, x, mu, k] == (site * 4 + mu) * 18 + k
+    with pytest.raises(ValueError):
+        read_conf(tmp_path / "c.bin", (2, 3, 4, 4))
+
+
+def test_input_list_sorted_bin_only(tmp_path):
+    for name in ["conf0002.bin", "conf0000.bin", "notes.txt", "conf0001.bin"]:
+        (tmp_path / name).write_bytes(b"")
+    assert [p.split("/")[-1] for p in get_input_list(tmp_path)] == ["conf0000.bin", "conf0001.bin", "conf0002.bin"]
