@@ -266,6 +266,13 @@ def our_arm(args, dist: Dist):
     dist.barrier()
     elapsed_ms, kernel_ms = f.time_steps(EPS, args.steps, kernels=False)
     dist.barrier()
+    if args.profile:
+        clocks.stop()
+        f.close()
+        if dist.rank == 0:
+            print(json.dumps({"profile": True, "precision": prec, "lattice": list(DIMS),
+                              "ms_per_step": elapsed_ms / args.steps}))
+        return
     # stage-kernel durations, measured with events around every launch of a second timed pass
     _, kernel_ms = f.time_steps(EPS, args.steps, kernels=True)
     clocks.stop()
@@ -375,7 +382,12 @@ def main():
     ap.add_argument("--precision", default="fp32_12", choices=["fp64", "fp32_18", "fp32_12"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--lattice", type=int, default=32, help="L of the L^4 lattice (profiling of smaller cases)")
+    ap.add_argument("--profile", action="store_true",
+                    help="only the warm-up and timed steps of one precision (for ncu captures)")
     args = ap.parse_args()
+    global DIMS
+    DIMS = (args.lattice,) * 4
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
