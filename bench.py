@@ -242,6 +242,43 @@ def reference_arm(args):
 # ----------------------------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------------------------
+def ensemble_sizes():
+    """The batched workload: 64 configurations, 16 each of 8^4, 12^4, 16^4 and 16^3 x 32."""
+    return [(8,) * 4] * 16 + [(12,) * 4] * 16 + [(16,) * 4] * 16 + [(16, 16, 16, 32)] * 16
+
+
+def ensemble_measure(prec: str, steps: int, dev: int):
+    """Aggregate link-updates/s of the batched ensemble (one persistent launch per
+    stage for all 64 configurations) against flowing them one by one."""
+    import numpy as np
+
+    from latticeyangmills_b200 import Ensemble, GluonField
+
+    sizes = ensemble_sizes()
+    rng = np.random.default_rng(4)
+    a_list = rng.uniform(0.25, 0.45, size=len(sizes))
+    links = sum(4 * s[0] * s[1] * s[2] * s[3] for s in sizes)
+    ens = Ensemble(sizes, prec, device=dev)
+    for c in range(len(sizes)):
+        ens.init_links(c, "expiah", float(a_list[c]), SEED + c, c)
+    block, grid = ens.autotune(EPS)
+    ens.time_steps(EPS, 3)
+    ms = ens.time_steps(EPS, steps)
+    ens.close()
+    one_ms = 0.0
+    for c, n in enumerate(sizes):
+        f = GluonField(n, prec, device=dev)
+        f.init_links("expiah", float(a_list[c]), SEED + c, c)
+        f.time_steps(EPS, 3)
+        el, _ = f.time_steps(EPS, steps)
+        one_ms += el
+        f.close()
+    return {"configs": len(sizes), "sizes": "16x8^4 + 16x12^4 + 16x16^4 + 16x16^3x32", "precision": prec,
+            "steps": steps, "link_updates_per_s": links * steps / (ms / 1e3),
+            "one_by_one_link_updates_per_s": links * steps / (one_ms / 1e3),
+            "speedup_vs_one_by_one": one_ms / ms, "autotuned": {"block": block, "grid": grid}}
+
+
 def our_arm(args, dist: Dist):
     import ctypes
 
@@ -333,6 +370,10 @@ def our_arm(args, dist: Dist):
     N.load().ymflow_host_free(host)
     rows_bytes = 2 * 48  # two measurement rows (before / after) come back per job
 
+    ensemble = None
+    if not args.skip_ensemble and dist.rank == 0:
+        ensemble = ensemble_measure(prec if prec != "fp64" else "fp32_18", args.steps, dev)
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.skip_cpu:
         val, detail = run_reference(DIMS, 1, 1)
@@ -366,6 +407,7 @@ def our_arm(args, dist: Dist):
                     "d2h_bytes_per_step": rows_bytes / args.steps,
                     "what": "per job: ymflow_upload of the .bin-layout FP64 field from pinned host memory, "
                             "ymflow_flow of K steps, observables rows back to the host"},
+            "ensemble": ensemble,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
@@ -382,6 +424,7 @@ def main():
     ap.add_argument("--precision", default="fp32_12", choices=["fp64", "fp32_18", "fp32_12"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--lattice", type=int, default=32, help="L of the L^4 lattice (profiling of smaller cases)")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps of one precision (for ncu captures)")

@@ -143,8 +143,10 @@ YMFLOW_API int ymflow_reset_time(ymflow_ctx* ctx);
 YMFLOW_API int ymflow_time_steps(ymflow_ctx* ctx, double eps, int nsteps, float* elapsed_ms, float* kernel_ms);
 
 /* Tuning knobs.  key YMFLOW_OPT_BLOCK: threads per block of the stage kernel
- * (32..256, multiple of 32); YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a
- * captured CUDA graph (default), 0 = plain launches. */
+ * (128 or 256: four warps, one per direction, per 32 sites); YMFLOW_OPT_OBS_BLOCK:
+ * threads per block of the observables kernel (32..256, multiple of 32);
+ * YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a captured CUDA graph
+ * (default), 0 = plain launches. */
 #define YMFLOW_OPT_BLOCK 1
 #define YMFLOW_OPT_GRAPH 2
 #define YMFLOW_OPT_OBS_BLOCK 3
@@ -157,6 +159,34 @@ YMFLOW_API int ymflow_host_free(void* ptr);
 
 /* Device bytes held by the context (links x2, force, staging, scratch). */
 YMFLOW_API int ymflow_device_bytes(const ymflow_ctx* ctx, int64_t* bytes);
+
+/* ---- batched ensemble --------------------------------------------------------------
+ * Many configurations, of any mix of lattice sizes, flowed together: every RK3
+ * stage of every configuration is one persistent launch over a work list of
+ * (configuration, block of sites), and each step is replayed as a captured CUDA
+ * graph.  Replaces the reference's one-by-one loop over the sorted InputDir
+ * files (src/Apps/wilsonflow.cpp:96-109).  Output rows are [row][conf]. */
+typedef struct ymflow_ens ymflow_ens;
+
+/* dims: nconf x 4 extents (x, y, z, t) per configuration. */
+YMFLOW_API ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, int device, int* status);
+YMFLOW_API void ymflow_ensemble_destroy(ymflow_ens* ens);
+YMFLOW_API const char* ymflow_ensemble_last_error(const ymflow_ens* ens);
+YMFLOW_API int ymflow_ensemble_upload(ymflow_ens* ens, int conf, const double* links_aos);
+YMFLOW_API int ymflow_ensemble_download(ymflow_ens* ens, int conf, double* links_aos);
+YMFLOW_API int ymflow_ensemble_init_links(ymflow_ens* ens, int conf, int kind, double a, uint64_t seed,
+                                          uint32_t config, double haar_frac);
+/* As ymflow_flow for every configuration at once; out holds rows_cap x nconf entries. */
+YMFLOW_API int ymflow_ensemble_flow(ymflow_ens* ens, double eps, int nsteps, int measure_every, int reunit_every,
+                                    ymflow_obs* out, int rows_cap, int* n_rows);
+YMFLOW_API int ymflow_ensemble_reset_time(ymflow_ens* ens);
+/* Device-timed RK3 steps of the whole ensemble (no measurements). */
+YMFLOW_API int ymflow_ensemble_time_steps(ymflow_ens* ens, double eps, int nsteps, float* elapsed_ms);
+/* Times the stage kernel over threads-per-block {128, 256} and persistent grids
+ * {one CTA per work item, 1x and 2x the resident CTAs}, keeps the fastest, and
+ * caches it for every ensemble of the same sizes and precision in the process.
+ * Does not change the flow state. */
+YMFLOW_API int ymflow_ensemble_autotune(ymflow_ens* ens, double eps, int* block, int* grid);
 
 #ifdef __cplusplus
 }

@@ -34,7 +34,13 @@ EXPORTS = (
     "ymflow_upload", "ymflow_download", "ymflow_init_links", "ymflow_observables", "ymflow_flow",
     "ymflow_derivative", "ymflow_su3_exp", "ymflow_reset_time", "ymflow_time_steps", "ymflow_set_option", "ymflow_get_option",
     "ymflow_host_alloc", "ymflow_host_free", "ymflow_device_bytes",
+    "ymflow_ensemble_create", "ymflow_ensemble_destroy", "ymflow_ensemble_last_error",
+    "ymflow_ensemble_upload", "ymflow_ensemble_download", "ymflow_ensemble_init_links",
+    "ymflow_ensemble_flow", "ymflow_ensemble_reset_time", "ymflow_ensemble_time_steps",
+    "ymflow_ensemble_autotune",
 )
+NON_INT = ("ymflow_version", "ymflow_create", "ymflow_destroy", "ymflow_last_error", "ymflow_ensemble_create",
+           "ymflow_ensemble_destroy", "ymflow_ensemble_last_error")
 
 
 class Obs(ctypes.Structure):
@@ -95,8 +101,24 @@ def load():
     l.ymflow_host_alloc.argtypes = [ctypes.c_int64, ctypes.POINTER(vp)]
     l.ymflow_host_free.argtypes = [vp]
     l.ymflow_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    IP = ctypes.POINTER(ctypes.c_int)
+    l.ymflow_ensemble_create.argtypes = [ctypes.c_int, IP, ctypes.c_int, ctypes.c_int, IP]
+    l.ymflow_ensemble_create.restype = vp
+    l.ymflow_ensemble_destroy.argtypes = [vp]
+    l.ymflow_ensemble_destroy.restype = None
+    l.ymflow_ensemble_last_error.argtypes = [vp]
+    l.ymflow_ensemble_last_error.restype = ctypes.c_char_p
+    l.ymflow_ensemble_upload.argtypes = [vp, ctypes.c_int, vp]
+    l.ymflow_ensemble_download.argtypes = [vp, ctypes.c_int, vp]
+    l.ymflow_ensemble_init_links.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_uint64,
+                                             ctypes.c_uint32, ctypes.c_double]
+    l.ymflow_ensemble_flow.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(Obs), ctypes.c_int, IP]
+    l.ymflow_ensemble_reset_time.argtypes = [vp]
+    l.ymflow_ensemble_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    l.ymflow_ensemble_autotune.argtypes = [vp, ctypes.c_double, IP, IP]
     for name in EXPORTS:
-        if name not in ("ymflow_version", "ymflow_create", "ymflow_destroy", "ymflow_last_error"):
+        if name not in NON_INT:
             getattr(l, name).restype = ctypes.c_int
     _lib = l
     return l

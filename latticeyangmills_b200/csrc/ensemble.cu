@@ -1,0 +1,595 @@
+// K6: batched ensemble.  Many configurations of uneven lattice sizes advance
+// through each RK3 stage in ONE persistent launch: the work list is every
+// (configuration, block of sites) pair, a fixed grid of CTAs walks it with a
+// grid-stride loop, and each item looks its configuration up in a prefix table.
+// The three stage launches of a step are replayed as a captured CUDA graph.
+// The reference flows its configurations one after another
+// (src/Apps/wilsonflow.cpp:96-109); small lattices cannot fill a B200 that way.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "api_util.h"
+#include "flow_device.cuh"
+#include "kernels.h"
+#include "ymflow.h"
+
+namespace ym {
+
+struct EnsConf {
+    Geo g;
+    int64_t uoff;  // start of this configuration in the link pool (bytes, 16-aligned)
+    int64_t zoff;  // start in the generator pool (bytes, 16-aligned)
+    int blk0;      // first work item
+    int nblk;      // work items (blocks of sites)
+};
+
+__device__ __forceinline__ int find_conf(const EnsConf* confs, int nconf, int item) {
+    int lo = 0, hi = nconf - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&confs[mid].blk0) <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class F, int STAGE>
+__global__ void __launch_bounds__(256) ens_stage_kernel(char* uin, char* uout, char* z,
+                                                         const EnsConf* __restrict__ confs, int nconf, int nitems,
+                                                         typename F::Real eps) {
+    using R = typename F::Real;
+    const int spb = blockDim.x >> 2;  // sites per block: four warps (directions) per 32 sites
+    const int w = threadIdx.x >> 5;
+    const int mu = w & 3;
+    const int lane_site = ((w >> 2) << 5) + (threadIdx.x & 31);
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const EnsConf& C = confs[find_conf(confs, nconf, item)];
+        const Geo g = C.g;
+        const int s = (item - C.blk0) * spb + lane_site;
+        if (s < g.V) {
+            const F in{uin + C.uoff, g.V}, out{uout + C.uoff, g.V};
+            const ForceField<R> zf{z + C.zoff, g.V};
+            rk_link_update<F, STAGE>(in, out, zf, g, eps, s, mu);
+        }
+    }
+}
+
+template <class F>
+static cudaError_t launch_ens_typed(int stage, void* uin, void* uout, void* z, const EnsConf* confs, int nconf,
+                                    int nitems, int grid, int block, double eps, cudaStream_t st) {
+    using R = typename F::Real;
+    const R e = R(stage == 0 ? eps * 0.25 : eps);
+    char *a = (char*)uin, *b = (char*)uout, *zz = (char*)z;
+    switch (stage) {
+        case 0: ens_stage_kernel<F, 0><<<grid, block, 0, st>>>(a, b, zz, confs, nconf, nitems, e); break;
+        case 1: ens_stage_kernel<F, 1><<<grid, block, 0, st>>>(a, b, zz, confs, nconf, nitems, e); break;
+        default: ens_stage_kernel<F, 2><<<grid, block, 0, st>>>(a, b, zz, confs, nconf, nitems, e); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ens_stage(int prec, int stage, void* uin, void* uout, void* z, const EnsConf* confs, int nconf,
+                             int nitems, int grid, int block, double eps, cudaStream_t st) {
+    switch (prec) {
+        case kFP64: return launch_ens_typed<FieldD18>(stage, uin, uout, z, confs, nconf, nitems, grid, block, eps, st);
+        case kFP32_18: return launch_ens_typed<FieldF18>(stage, uin, uout, z, confs, nconf, nitems, grid, block, eps, st);
+        case kFP32_12: return launch_ens_typed<FieldF12>(stage, uin, uout, z, confs, nconf, nitems, grid, block, eps, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int ens_max_resident(int prec, int block) {
+    int n = 0;
+    cudaError_t e = cudaSuccess;
+    switch (prec) {
+        case kFP64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_stage_kernel<FieldD18, 1>, block, 0); break;
+        case kFP32_18: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_stage_kernel<FieldF18, 1>, block, 0); break;
+        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_stage_kernel<FieldF12, 1>, block, 0); break;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return std::max(n, 1);
+}
+
+// Tuning results shared by every ensemble with the same signature in this process.
+std::mutex g_tune_mu;
+std::map<std::string, std::pair<int, int>> g_tune_cache;
+
+}  // namespace ym
+
+using namespace ym;
+
+struct ymflow_ens {
+    int nconf = 0;
+    int prec = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<EnsConf> confs;  // host copy
+    EnsConf* confs_dev = nullptr;
+    void* u[2] = {nullptr, nullptr};
+    int cur = 0;
+    void* z = nullptr;
+    int64_t pool_links = 0;  // bytes per link pool
+    int64_t pool_force = 0;  // bytes of the generator pool
+    double* staging = nullptr;  // .bin-layout buffer sized for the largest configuration
+    int64_t max_v = 0;
+    double* partials = nullptr;
+    int partial_cap = 0;
+    double* meas = nullptr;
+    int meas_cap = 0;
+    double* meas_host = nullptr;
+    unsigned long long* deviation = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    double graph_eps[2] = {0.0, 0.0};
+    int graph_cfg[2][2] = {{0, 0}, {0, 0}};
+    int block = 128;
+    int grid = 0;  // persistent CTAs (0: one per work item)
+    int obs_block = 128;
+    bool use_graph = true;
+    bool tuned = false;
+    std::vector<char> loaded;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t step = 0;
+    double t = 0.0;
+    std::string err;
+    std::string signature;
+};
+
+namespace {
+
+thread_local std::string g_ens_create_error;
+
+int efail(ymflow_ens* e, int code, const std::string& m) {
+    if (e) e->err = m;
+    return code;
+}
+int ecuda(ymflow_ens* e, cudaError_t c, const char* what) { return efail(e, status_of(c), cuda_message(c, what)); }
+
+#define YE_CK(ens, call, what)                                     \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return ecuda(ens, e_, what);        \
+    } while (0)
+
+// Rebuild the work-list prefix table for a block size and upload it.
+int set_block(ymflow_ens* e, int block) {
+    const int spb = block / 4;
+    int blk = 0;
+    for (EnsConf& c : e->confs) {
+        c.blk0 = blk;
+        c.nblk = int((c.g.V + spb - 1) / spb);
+        blk += c.nblk;
+    }
+    YE_CK(e, cudaMemcpyAsync(e->confs_dev, e->confs.data(), sizeof(EnsConf) * e->confs.size(),
+                             cudaMemcpyHostToDevice, e->stream),
+          "work list upload");
+    YE_CK(e, cudaStreamSynchronize(e->stream), "work list upload");
+    e->block = block;
+    return YMFLOW_OK;
+}
+
+int nitems(const ymflow_ens* e) {
+    return e->confs.empty() ? 0 : e->confs.back().blk0 + e->confs.back().nblk;
+}
+
+cudaError_t enqueue_ens_step(ymflow_ens* e, int from, double eps) {
+    void* a = e->u[from];
+    void* b = e->u[1 - from];
+    void* in[3] = {a, b, a};
+    void* out[3] = {b, a, b};
+    const int ni = nitems(e);
+    const int grid = e->grid > 0 ? std::min(e->grid, ni) : ni;
+    for (int s = 0; s < 3; s++) {
+        cudaError_t r = launch_ens_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf, ni, grid, e->block,
+                                         eps, e->stream);
+        if (r != cudaSuccess) return r;
+    }
+    return cudaSuccess;
+}
+
+void drop_graphs(ymflow_ens* e) {
+    for (int i = 0; i < 2; i++) {
+        if (e->graph[i]) cudaGraphExecDestroy(e->graph[i]);
+        e->graph[i] = nullptr;
+    }
+}
+
+int run_ens_step(ymflow_ens* e, double eps) {
+    const int from = e->cur;
+    if (e->use_graph) {
+        if (!e->graph[from] || e->graph_eps[from] != eps || e->graph_cfg[from][0] != e->block ||
+            e->graph_cfg[from][1] != e->grid) {
+            if (e->graph[from]) cudaGraphExecDestroy(e->graph[from]);
+            e->graph[from] = nullptr;
+            cudaGraph_t g = nullptr;
+            YE_CK(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            cudaError_t le = enqueue_ens_step(e, from, eps);
+            cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+            if (le != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return ecuda(e, le, "stage launch during capture");
+            }
+            YE_CK(e, ce, "end capture");
+            cudaError_t ie = cudaGraphInstantiate(&e->graph[from], g, 0);
+            cudaGraphDestroy(g);
+            YE_CK(e, ie, "instantiate step graph");
+            e->graph_eps[from] = eps;
+            e->graph_cfg[from][0] = e->block;
+            e->graph_cfg[from][1] = e->grid;
+        }
+        YE_CK(e, cudaGraphLaunch(e->graph[from], e->stream), "launch step graph");
+    } else {
+        YE_CK(e, enqueue_ens_step(e, from, eps), "stage launch");
+    }
+    e->cur = 1 - from;
+    return YMFLOW_OK;
+}
+
+int ens_alloc(ymflow_ens* e, void** p, size_t bytes, const char* what) {
+    cudaError_t c = cudaMalloc(p, bytes);
+    if (c != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return ecuda(e, c, what);
+    }
+    return YMFLOW_OK;
+}
+
+int ensure_ens_meas(ymflow_ens* e, int rows) {
+    const int need = rows * e->nconf;
+    if (need <= e->meas_cap) return YMFLOW_OK;
+    if (e->meas) cudaFree(e->meas);
+    if (e->meas_host) cudaFreeHost(e->meas_host);
+    e->meas = nullptr;
+    e->meas_host = nullptr;
+    e->meas_cap = 0;
+    int r = ens_alloc(e, (void**)&e->meas, size_t(need) * 4 * sizeof(double), "measurement rows");
+    if (r != YMFLOW_OK) return r;
+    YE_CK(e, cudaMallocHost((void**)&e->meas_host, size_t(need) * 4 * sizeof(double)), "pinned rows");
+    e->meas_cap = need;
+    return YMFLOW_OK;
+}
+
+// Observables of every configuration into rows [row*nconf, row*nconf + nconf).
+int enqueue_ens_measure(ymflow_ens* e, int row) {
+    for (int c = 0; c < e->nconf; c++) {
+        const EnsConf& C = e->confs[c];
+        const void* u = (const char*)e->u[e->cur] + C.uoff;
+        YE_CK(e, launch_observables(e->prec, u, C.g, e->partials, e->obs_block, e->stream), "observables launch");
+        YE_CK(e, launch_obs_finalize(e->partials, obs_blocks(C.g, e->obs_block), C.g,
+                                     e->meas + 4 * (size_t(row) * e->nconf + c), e->stream),
+              "observables fold");
+    }
+    return YMFLOW_OK;
+}
+
+void* conf_links(const ymflow_ens* e, int c) { return (char*)e->u[e->cur] + e->confs[c].uoff; }
+
+float time_stage0(ymflow_ens* e, double eps, int reps) {
+    // stage 0 reads u[cur] and writes only u[1-cur] and z, which the next step
+    // overwrites anyway, so tuning does not disturb the flow state
+    const int ni = nitems(e);
+    const int grid = e->grid > 0 ? std::min(e->grid, ni) : ni;
+    launch_ens_stage(e->prec, 0, e->u[e->cur], e->u[1 - e->cur], e->z, e->confs_dev, e->nconf, ni, grid, e->block,
+                     eps, e->stream);
+    cudaEventRecord(e->ev0, e->stream);
+    for (int i = 0; i < reps; i++)
+        launch_ens_stage(e->prec, 0, e->u[e->cur], e->u[1 - e->cur], e->z, e->confs_dev, e->nconf, ni, grid,
+                         e->block, eps, e->stream);
+    cudaEventRecord(e->ev1, e->stream);
+    if (cudaEventSynchronize(e->ev1) != cudaSuccess) return -1.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    return ms / float(reps);
+}
+
+}  // namespace
+
+extern "C" {
+
+ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, int device, int* status) {
+    auto set = [&](int s, const std::string& m) {
+        if (status) *status = s;
+        g_ens_create_error = m;
+    };
+    if (nconf < 1 || !dims) {
+        set(YMFLOW_ERR_ARG, "need at least one configuration and its dims");
+        return nullptr;
+    }
+    if (precision < YMFLOW_FP64 || precision > YMFLOW_FP32_12) {
+        set(YMFLOW_ERR_ARG, "unknown precision");
+        return nullptr;
+    }
+    std::string why;
+    if (!device_usable(device, &why)) {
+        set(YMFLOW_ERR_NODEVICE, why);
+        return nullptr;
+    }
+    ymflow_ens* e = new (std::nothrow) ymflow_ens();
+    if (!e) {
+        set(YMFLOW_ERR_OOM, "host allocation failed");
+        return nullptr;
+    }
+    DeviceGuard guard(device);
+    e->nconf = nconf;
+    e->prec = precision;
+    e->device = device;
+    e->confs.resize(nconf);
+    e->loaded.assign(nconf, 0);
+    int64_t uo = 0, zo = 0;
+    for (int c = 0; c < nconf; c++) {
+        const int* d = dims + 4 * c;
+        int64_t V = 1;
+        for (int i = 0; i < 4; i++) {
+            if (d[i] < 1 || d[i] > 4096) {
+                set(YMFLOW_ERR_ARG, "configuration " + std::to_string(c) + ": extents must be in 1..4096");
+                delete e;
+                return nullptr;
+            }
+            V *= d[i];
+        }
+        if (V >= (int64_t(1) << 31)) {
+            set(YMFLOW_ERR_ARG, "configuration " + std::to_string(c) + ": volume must be below 2^31 sites");
+            delete e;
+            return nullptr;
+        }
+        EnsConf& C = e->confs[c];
+        C.g = make_geo(d);
+        C.uoff = uo;
+        C.zoff = zo;
+        uo += int64_t(4) * int64_t(link_bytes(precision)) * V;
+        zo += int64_t(4) * int64_t(force_bytes(precision)) * V;
+        e->max_v = std::max(e->max_v, V);
+        e->signature += std::to_string(d[0]) + "x" + std::to_string(d[1]) + "x" + std::to_string(d[2]) + "x" +
+                        std::to_string(d[3]) + ";";
+    }
+    e->signature += "p" + std::to_string(precision);
+    e->pool_links = uo;
+    e->pool_force = zo;
+    int r = YMFLOW_OK;
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) r = YMFLOW_ERR_CUDA;
+    if (r == YMFLOW_OK) r = ens_alloc(e, &e->u[0], size_t(uo), "link pool 0");
+    if (r == YMFLOW_OK) r = ens_alloc(e, &e->u[1], size_t(uo), "link pool 1");
+    if (r == YMFLOW_OK) r = ens_alloc(e, &e->z, size_t(zo), "generator pool");
+    if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->confs_dev, sizeof(EnsConf) * nconf, "work list");
+    if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->deviation, sizeof(unsigned long long), "drift flag");
+    if (r == YMFLOW_OK) {
+        Geo gmax{};
+        gmax.V = e->max_v;
+        e->partial_cap = std::max(obs_blocks(gmax, 32), 1);
+        r = ens_alloc(e, (void**)&e->partials, size_t(e->partial_cap) * 3 * sizeof(double), "partials");
+    }
+    if (r == YMFLOW_OK && (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess))
+        r = YMFLOW_ERR_CUDA;
+    if (r == YMFLOW_OK) r = set_block(e, 128);
+    if (r == YMFLOW_OK) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(e->signature);
+        if (it != g_tune_cache.end()) {
+            e->grid = it->second.second;
+            r = set_block(e, it->second.first);
+            e->tuned = true;
+        }
+    }
+    if (r != YMFLOW_OK) {
+        set(r, e->err.empty() ? "ensemble setup failed" : e->err);
+        ymflow_ensemble_destroy(e);
+        return nullptr;
+    }
+    if (status) *status = YMFLOW_OK;
+    return e;
+}
+
+void ymflow_ensemble_destroy(ymflow_ens* e) {
+    if (!e) return;
+    DeviceGuard guard(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    drop_graphs(e);
+    for (void* p : {e->u[0], e->u[1], e->z, (void*)e->confs_dev, (void*)e->staging, (void*)e->partials,
+                    (void*)e->meas, (void*)e->deviation})
+        if (p) cudaFree(p);
+    if (e->meas_host) cudaFreeHost(e->meas_host);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+const char* ymflow_ensemble_last_error(const ymflow_ens* e) { return e ? e->err.c_str() : g_ens_create_error.c_str(); }
+
+int ymflow_ensemble_upload(ymflow_ens* e, int conf, const double* links) {
+    if (!e || !links || conf < 0 || conf >= e->nconf) return efail(e, YMFLOW_ERR_ARG, "bad argument to upload");
+    DeviceGuard guard(e->device);
+    if (!e->staging) {
+        int r = ens_alloc(e, (void**)&e->staging, size_t(e->max_v) * 4 * 18 * sizeof(double), "staging buffer");
+        if (r != YMFLOW_OK) return r;
+    }
+    const EnsConf& C = e->confs[conf];
+    YE_CK(e, cudaMemcpyAsync(e->staging, links, size_t(C.g.V) * 72 * sizeof(double), cudaMemcpyHostToDevice,
+                             e->stream),
+          "upload copy");
+    YE_CK(e, launch_pack(e->prec, e->staging, conf_links(e, conf), C.g, e->stream), "pack");
+    YE_CK(e, cudaStreamSynchronize(e->stream), "upload");
+    e->loaded[conf] = 1;
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_download(ymflow_ens* e, int conf, double* links) {
+    if (!e || !links || conf < 0 || conf >= e->nconf) return efail(e, YMFLOW_ERR_ARG, "bad argument to download");
+    if (!e->loaded[conf]) return efail(e, YMFLOW_ERR_STATE, "configuration not loaded");
+    DeviceGuard guard(e->device);
+    if (!e->staging) {
+        int r = ens_alloc(e, (void**)&e->staging, size_t(e->max_v) * 4 * 18 * sizeof(double), "staging buffer");
+        if (r != YMFLOW_OK) return r;
+    }
+    const EnsConf& C = e->confs[conf];
+    YE_CK(e, launch_unpack(e->prec, conf_links(e, conf), e->staging, C.g, e->stream), "unpack");
+    YE_CK(e, cudaMemcpyAsync(links, e->staging, size_t(C.g.V) * 72 * sizeof(double), cudaMemcpyDeviceToHost,
+                             e->stream),
+          "download copy");
+    YE_CK(e, cudaStreamSynchronize(e->stream), "download");
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_init_links(ymflow_ens* e, int conf, int kind, double a, uint64_t seed, uint32_t config,
+                               double haar_frac) {
+    if (!e || conf < 0 || conf >= e->nconf) return efail(e, YMFLOW_ERR_ARG, "bad configuration index");
+    if (kind != YMFLOW_FIELD_COLD && kind != YMFLOW_FIELD_EXPIAH) return efail(e, YMFLOW_ERR_ARG, "unknown kind");
+    DeviceGuard guard(e->device);
+    const EnsConf& C = e->confs[conf];
+    YE_CK(e, launch_init_links(e->prec, conf_links(e, conf), C.g, kind == YMFLOW_FIELD_COLD ? kCold : kExpIAH, a,
+                               seed, config, e->stream),
+          "init");
+    if (haar_frac > 0.0)
+        YE_CK(e, launch_haar_mix(e->prec, conf_links(e, conf), C.g, haar_frac, seed, config, e->stream), "haar");
+    YE_CK(e, cudaStreamSynchronize(e->stream), "init links");
+    e->loaded[conf] = 1;
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_flow(ymflow_ens* e, double eps, int nsteps, int measure_every, int reunit_every,
+                         ymflow_obs* out, int rows_cap, int* n_rows) {
+    if (!e) return YMFLOW_ERR_ARG;
+    if (n_rows) *n_rows = 0;
+    if (nsteps < 0) return efail(e, YMFLOW_ERR_ARG, "nsteps < 0");
+    for (int c = 0; c < e->nconf; c++)
+        if (!e->loaded[c]) return efail(e, YMFLOW_ERR_STATE, "configuration " + std::to_string(c) + " not loaded");
+    int rows = 1;
+    for (int s = 1; s <= nsteps; s++)
+        if ((measure_every > 0 && s % measure_every == 0) || s == nsteps) rows++;
+    if (out && rows_cap < rows) return efail(e, YMFLOW_ERR_CAPACITY, "output holds too few rows");
+    DeviceGuard guard(e->device);
+    int r = ensure_ens_meas(e, rows);
+    if (r != YMFLOW_OK) return r;
+    std::vector<int64_t> rs(rows);
+    std::vector<double> rt(rows);
+    const bool reunit = e->prec != YMFLOW_FP64 && reunit_every > 0;
+    if (reunit) YE_CK(e, cudaMemsetAsync(e->deviation, 0, sizeof(unsigned long long), e->stream), "reset drift");
+    int row = 0;
+    if ((r = enqueue_ens_measure(e, row)) != YMFLOW_OK) return r;
+    rs[row] = e->step;
+    rt[row] = e->t;
+    row++;
+    for (int s = 1; s <= nsteps; s++) {
+        if ((r = run_ens_step(e, eps)) != YMFLOW_OK) return r;
+        e->step++;
+        e->t += eps;
+        if (reunit && s % reunit_every == 0)
+            for (int c = 0; c < e->nconf; c++)
+                YE_CK(e, launch_reunitarize(e->prec, conf_links(e, c), e->confs[c].g, e->deviation, e->stream),
+                      "reunitarise");
+        if ((measure_every > 0 && s % measure_every == 0) || s == nsteps) {
+            if ((r = enqueue_ens_measure(e, row)) != YMFLOW_OK) return r;
+            rs[row] = e->step;
+            rt[row] = e->t;
+            row++;
+        }
+    }
+    YE_CK(e, cudaMemcpyAsync(e->meas_host, e->meas, size_t(rows) * e->nconf * 4 * sizeof(double),
+                             cudaMemcpyDeviceToHost, e->stream),
+          "rows copy");
+    unsigned long long bits = 0;
+    if (reunit)
+        YE_CK(e, cudaMemcpyAsync(&bits, e->deviation, sizeof(bits), cudaMemcpyDeviceToHost, e->stream), "drift copy");
+    YE_CK(e, cudaStreamSynchronize(e->stream), "ensemble flow");
+    bool nonfinite = false;
+    for (int i = 0; i < rows; i++)
+        for (int c = 0; c < e->nconf; c++) {
+            const double* m = e->meas_host + 4 * (size_t(i) * e->nconf + c);
+            if (out) {
+                ymflow_obs& o = out[size_t(i) * e->nconf + c];
+                o.step = int32_t(rs[i]);
+                o.pad = 0;
+                o.t = rt[i];
+                o.plaq = m[0];
+                o.topc = m[1];
+                o.energy = m[2];
+                o.t2E = -rt[i] * rt[i] * m[2] / (64.0 * double(e->confs[c].g.V));
+            }
+            if (m[3] != 0.0) nonfinite = true;
+        }
+    if (n_rows) *n_rows = rows;
+    if (nonfinite) return efail(e, YMFLOW_ERR_NONFINITE, "non-finite observable during the ensemble flow");
+    if (reunit) {
+        double d;
+        std::memcpy(&d, &bits, sizeof(d));
+        if (d > 1e-3) return efail(e, YMFLOW_ERR_UNITARITY, "links drifted from SU(3)");
+    }
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_time_steps(ymflow_ens* e, double eps, int nsteps, float* elapsed_ms) {
+    if (!e || !elapsed_ms || nsteps < 1) return efail(e, YMFLOW_ERR_ARG, "bad argument to time_steps");
+    for (int c = 0; c < e->nconf; c++)
+        if (!e->loaded[c]) return efail(e, YMFLOW_ERR_STATE, "configuration not loaded");
+    DeviceGuard guard(e->device);
+    YE_CK(e, cudaEventRecord(e->ev0, e->stream), "event");
+    for (int s = 0; s < nsteps; s++) {
+        int r = run_ens_step(e, eps);
+        if (r != YMFLOW_OK) return r;
+        e->step++;
+        e->t += eps;
+    }
+    YE_CK(e, cudaEventRecord(e->ev1, e->stream), "event");
+    YE_CK(e, cudaEventSynchronize(e->ev1), "timed steps");
+    YE_CK(e, cudaEventElapsedTime(elapsed_ms, e->ev0, e->ev1), "elapsed");
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* grid_out) {
+    if (!e) return YMFLOW_ERR_ARG;
+    for (int c = 0; c < e->nconf; c++)
+        if (!e->loaded[c]) return efail(e, YMFLOW_ERR_STATE, "configuration not loaded");
+    DeviceGuard guard(e->device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+    float best = 1e30f;
+    int best_block = e->block, best_grid = e->grid;
+    for (int block : {128, 256}) {
+        int r = set_block(e, block);
+        if (r != YMFLOW_OK) return r;
+        const int resident = ens_max_resident(e->prec, block);
+        for (int grid : {0, resident * sms, 2 * resident * sms}) {
+            e->grid = grid;
+            const float ms = time_stage0(e, eps, 3);
+            if (ms < 0.f) return ecuda(e, cudaGetLastError(), "tuning launch");
+            if (ms < best) {
+                best = ms;
+                best_block = block;
+                best_grid = grid;
+            }
+        }
+    }
+    e->grid = best_grid;
+    int r = set_block(e, best_block);
+    if (r != YMFLOW_OK) return r;
+    drop_graphs(e);
+    e->tuned = true;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[e->signature] = {best_block, best_grid};
+    }
+    if (block_out) *block_out = best_block;
+    if (grid_out) *grid_out = best_grid;
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_reset_time(ymflow_ens* e) {
+    if (!e) return YMFLOW_ERR_ARG;
+    e->step = 0;
+    e->t = 0.0;
+    return YMFLOW_OK;
+}
+
+}  // extern "C"

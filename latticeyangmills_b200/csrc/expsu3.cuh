@@ -183,4 +183,23 @@ __device__ __forceinline__ void exp_iq(const Herm8<R>& q, M3<R>& e) {
 #undef YM_OFFD
 }
 
+// Rows 0 and 1 of e^{iQ} (enough to update an SU(3) link through its first two rows).
+template <class R>
+__device__ __forceinline__ void exp_iq_rows2(const Herm8<R>& q, Rows2<R>& e) {
+    const R q22 = -(q.d0 + q.d1);
+    const ChCoef<R> f = exp_coefficients<R>(q, q22);
+    const QSquared<R> s = q_squared(q, q22);
+    e.e[0][0] = cx(f.f0.re + f.f1.re * q.d0 + f.f2.re * s.a00, f.f0.im + f.f1.im * q.d0 + f.f2.im * s.a00);
+    e.e[1][1] = cx(f.f0.re + f.f1.re * q.d1 + f.f2.re * s.a11, f.f0.im + f.f1.im * q.d1 + f.f2.im * s.a11);
+    // upper entries f1 q_ij + f2 (Q^2)_ij; e10 from the conjugates of q01 and (Q^2)_01
+    e.e[0][1] = cx(f.f1.re * q.z01.re - f.f1.im * q.z01.im + f.f2.re * s.a01.re - f.f2.im * s.a01.im,
+                   f.f1.re * q.z01.im + f.f1.im * q.z01.re + f.f2.re * s.a01.im + f.f2.im * s.a01.re);
+    e.e[0][2] = cx(f.f1.re * q.z02.re - f.f1.im * q.z02.im + f.f2.re * s.a02.re - f.f2.im * s.a02.im,
+                   f.f1.re * q.z02.im + f.f1.im * q.z02.re + f.f2.re * s.a02.im + f.f2.im * s.a02.re);
+    e.e[1][2] = cx(f.f1.re * q.z12.re - f.f1.im * q.z12.im + f.f2.re * s.a12.re - f.f2.im * s.a12.im,
+                   f.f1.re * q.z12.im + f.f1.im * q.z12.re + f.f2.re * s.a12.im + f.f2.im * s.a12.re);
+    e.e[1][0] = cx(f.f1.re * q.z01.re + f.f1.im * q.z01.im + f.f2.re * s.a01.re + f.f2.im * s.a01.im,
+                   -f.f1.re * q.z01.im + f.f1.im * q.z01.re - f.f2.re * s.a01.im + f.f2.im * s.a01.re);
+}
+
 }  // namespace ym

@@ -1,16 +1,20 @@
 // Device storage of gauge fields and flow generators, and the lattice geometry.
 //
-// HBM layout (structure of arrays, one plane per link direction and matrix
-// element so that a warp's 32 consecutive sites load 32 consecutive vectors):
+// HBM layout: structure of arrays, so that a warp's 32 consecutive sites read
+// 32 consecutive 16-byte vectors per load instruction.
 //
-//   links  U[mu][e][site]   e = complex element, row-major (9 stored, or 6 for the
-//                           two-row "12-real" form whose third row is rebuilt);
-//                           each entry a double2 (FP64) or float2 (FP32) (re, im)
-//   force  Z[mu][k][site]   the Hermitian traceless generator as 8 reals
-//                           (Herm8: Z00, Z11, Re/Im Z01, Re/Im Z02, Re/Im Z12)
+//   FP64 links   double2 plane per (mu, element e): 9 planes of V entries per mu
+//   FP32 links   float4 plane per (mu, element pair): elements (0,1) (2,3) (4,5)
+//                for the two-row 12-real form (3 planes per mu); the 18-real form
+//                adds (6,7) and a float2 plane for element 8 (placed after all
+//                float4 planes so every plane stays 16-byte aligned)
+//   generator    the Hermitian traceless Z as 8 reals (Herm8: Z00, Z11, Re/Im Z01,
+//                Z02, Z12): 4 double2 or 2 float4 planes per mu
 //
-// Site order is the reference's lexicographic order, x fastest
-// (include/Math/lattice.h:87-89), so the .bin byte order maps one-to-one.
+// Elements are row-major, (re, im); the two-row form stores rows 0 and 1 and
+// rebuilds row 2 = conj(row0 x row1) on load.  Site order is the reference's
+// lexicographic order, x fastest (include/Math/lattice.h:87-89), so the .bin
+// byte order maps one-to-one.  Site indices are 32-bit (V < 2^31).
 #pragma once
 #include <cstdint>
 
@@ -18,80 +22,198 @@
 
 namespace ym {
 
-template <class R>
-struct Vec2;
-template <>
-struct Vec2<double> {
-    using T = double2;
-};
-template <>
-struct Vec2<float> {
-    using T = float2;
+// Division of a site index (< 2^31) by a lattice extent d <= 4096 with one
+// multiply: q = (x * m) >> (32 + l), m = floor(2^(32+l)/d) + 1, l = ceil(log2 d)
+// (Granlund & Montgomery, PLDI 1994, Thm 4.2 with N = 32; x * m < 2^64 here).
+struct FastDiv {
+    uint64_t m;
+    int l;
 };
 
-// Periodic 4-D lattice in lexicographic order.  Coordinates are recovered by
-// division once per thread; neighbours are index offsets with wrap-around,
-// replacing the reference's whole-field shift() with its MPI self-exchange
+inline FastDiv make_fastdiv(int d) {
+    int l = 0;
+    while ((1 << l) < d) l++;
+    FastDiv f;
+    f.m = ((uint64_t(1) << (32 + l)) / uint64_t(d)) + 1;
+    f.l = l;
+    return f;
+}
+
+// Periodic 4-D lattice in lexicographic order.  Coordinates are recovered once
+// per thread; neighbours are index offsets with wrap-around, replacing the
+// reference's whole-field shift() with its MPI self-exchange
 // (include/Math/lattice.h:360-594).
 struct Geo {
     int n[4];
-    int64_t stride[4];  // 1, nx, nx*ny, nx*ny*nz
-    int64_t V;
+    int stride[4];  // 1, nx, nx*ny, nx*ny*nz
+    int V;
+    FastDiv div[3];  // by n[0], n[1], n[2]
 
-    __device__ __forceinline__ void coords(int64_t s, int c[4]) const {
-        int64_t r = s;
-        c[0] = int(r % n[0]);
-        r /= n[0];
-        c[1] = int(r % n[1]);
-        r /= n[1];
-        c[2] = int(r % n[2]);
-        c[3] = int(r / n[2]);
+    __device__ __forceinline__ static int fdiv(int x, const FastDiv& f) {
+        return int((uint64_t(uint32_t(x)) * f.m) >> (32 + f.l));
+    }
+    __device__ __forceinline__ void coords(int s, int c[4]) const {
+        const int q0 = fdiv(s, div[0]);
+        c[0] = s - q0 * n[0];
+        const int q1 = fdiv(q0, div[1]);
+        c[1] = q0 - q1 * n[1];
+        const int q2 = fdiv(q1, div[2]);
+        c[2] = q1 - q2 * n[2];
+        c[3] = q2;
     }
     // index of the site one step from (s, c) along d (dir = +1 or -1)
-    __device__ __forceinline__ int64_t hop(int64_t s, const int c[4], int d, int dir) const {
-        if (dir > 0) return c[d] == n[d] - 1 ? s - int64_t(n[d] - 1) * stride[d] : s + stride[d];
-        return c[d] == 0 ? s + int64_t(n[d] - 1) * stride[d] : s - stride[d];
+    __device__ __forceinline__ int hop(int s, const int c[4], int d, int dir) const {
+        if (dir > 0) return c[d] == n[d] - 1 ? s - (n[d] - 1) * stride[d] : s + stride[d];
+        return c[d] == 0 ? s + (n[d] - 1) * stride[d] : s - stride[d];
     }
-    // c[d] after one step along d
-    __device__ __forceinline__ int step_coord(int cd, int d, int dir) const {
-        if (dir > 0) return cd == n[d] - 1 ? 0 : cd + 1;
-        return cd == 0 ? n[d] - 1 : cd - 1;
+    // the same with a direction known only at run time (warp-uniform): the
+    // coordinate, extent and stride are picked by selects (no dynamic register
+    // or parameter indexing, which would go through local memory)
+    __device__ __forceinline__ int coord(const int c[4], int d) const {
+        return d == 0 ? c[0] : (d == 1 ? c[1] : (d == 2 ? c[2] : c[3]));
     }
-    // index after a step along d1 then a step along d2 (d1 != d2)
-    __device__ __forceinline__ int64_t hop2(int64_t s, const int c[4], int d1, int dir1, int d2, int dir2) const {
-        const int64_t s1 = hop(s, c, d1, dir1);
-        return hop(s1, c, d2, dir2);  // c[d2] unchanged by the first step
+    __device__ __forceinline__ int ext(int d) const {
+        return d == 0 ? n[0] : (d == 1 ? n[1] : (d == 2 ? n[2] : n[3]));
+    }
+    __device__ __forceinline__ int str(int d) const {
+        return d == 0 ? stride[0] : (d == 1 ? stride[1] : (d == 2 ? stride[2] : stride[3]));
+    }
+    __device__ __forceinline__ int hop_rt(int s, int cd, int d, int dir) const {
+        const int nd = ext(d);
+        const int sd = str(d);
+        if (dir > 0) return cd == nd - 1 ? s - (nd - 1) * sd : s + sd;
+        return cd == 0 ? s + (nd - 1) * sd : s - sd;
     }
 };
 
+inline Geo make_geo(const int dims[4]) {
+    Geo g;
+    for (int i = 0; i < 4; i++) g.n[i] = dims[i];
+    g.stride[0] = 1;
+    g.stride[1] = dims[0];
+    g.stride[2] = dims[0] * dims[1];
+    g.stride[3] = dims[0] * dims[1] * dims[2];
+    g.V = dims[0] * dims[1] * dims[2] * dims[3];
+    for (int i = 0; i < 3; i++) g.div[i] = make_fastdiv(dims[i]);
+    return g;
+}
+
+template <class R>
+__device__ __forceinline__ void set_elem(M3<R>& a, int e, R re, R im) {
+    a.e[e / 3][e % 3] = cx(re, im);
+}
+
 // Link field of NE stored complex elements per link (9: full, 6: two rows).
 template <class R, int NE>
-struct LinkField {
-    using Real = R;
-    using V2 = typename Vec2<R>::T;
-    static constexpr int kElems = NE;
-    V2* p;
-    int64_t V;
+struct LinkField;
 
-    __device__ __forceinline__ M3<R> load(int mu, int64_t s) const {
-        M3<R> a;
-        const V2* b = p + int64_t(mu) * NE * V + s;
+template <int NE>
+struct LinkField<double, NE> {
+    using Real = double;
+    static constexpr int kElems = NE;
+    void* p;
+    int V;
+
+    __device__ __forceinline__ const double2* plane(int mu, int e) const {
+        return reinterpret_cast<const double2*>(p) + int64_t(mu * NE + e) * V;
+    }
+    __device__ __forceinline__ Rows2<double> load_rows2(int mu, int s) const {
+        Rows2<double> a;
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            const double2 v = __ldg(plane(mu, e) + s);
+            a.e[e / 3][e % 3] = cx(v.x, v.y);
+        }
+        return a;
+    }
+    __device__ __forceinline__ M3<double> load(int mu, int s) const {
+        M3<double> a;
 #pragma unroll
         for (int e = 0; e < NE; e++) {
-            const V2 v = __ldg(b + int64_t(e) * V);
-            a.e[e / 3][e % 3] = cx(R(v.x), R(v.y));
+            const double2 v = __ldg(plane(mu, e) + s);
+            set_elem(a, e, v.x, v.y);
         }
         if (NE == 6) reconstruct_row2(a);
         return a;
     }
-    __device__ __forceinline__ void store(int mu, int64_t s, const M3<R>& a) const {
-        V2* b = p + int64_t(mu) * NE * V + s;
+    __device__ __forceinline__ void put(int mu, int e, int s, Cx<double> v) const {
+        double2* q = const_cast<double2*>(plane(mu, e)) + s;
+        *q = make_double2(v.re, v.im);
+    }
+    __device__ __forceinline__ void store(int mu, int s, const M3<double>& a) const {
 #pragma unroll
-        for (int e = 0; e < NE; e++) {
-            V2 v;
-            v.x = a.e[e / 3][e % 3].re;
-            v.y = a.e[e / 3][e % 3].im;
-            b[int64_t(e) * V] = v;
+        for (int e = 0; e < NE; e++) put(mu, e, s, a.e[e / 3][e % 3]);
+    }
+    __device__ __forceinline__ void store_rows2(int mu, int s, const Rows2<double>& a) const {
+#pragma unroll
+        for (int e = 0; e < 6; e++) put(mu, e, s, a.e[e / 3][e % 3]);
+        if (NE == 9) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) put(mu, 6 + k, s, row2_entry(a, k));
+        }
+    }
+};
+
+template <int NE>
+struct LinkField<float, NE> {
+    using Real = float;
+    static constexpr int kElems = NE;
+    static constexpr int kPairs = NE / 2;  // float4 planes per mu: 3 (12-real) or 4 (18-real)
+    void* p;
+    int V;
+
+    __device__ __forceinline__ const float4* pair(int mu, int k) const {
+        return reinterpret_cast<const float4*>(p) + int64_t(mu * kPairs + k) * V;
+    }
+    // element 8 of the 18-real form, after all float4 planes
+    __device__ __forceinline__ const float2* tail(int mu) const {
+        return reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(p) + int64_t(4 * kPairs) * V) +
+               int64_t(mu) * V;
+    }
+    __device__ __forceinline__ Rows2<float> load_rows2(int mu, int s) const {
+        Rows2<float> a;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float4 v = __ldg(pair(mu, k) + s);
+            a.e[(2 * k) / 3][(2 * k) % 3] = cx(v.x, v.y);
+            a.e[(2 * k + 1) / 3][(2 * k + 1) % 3] = cx(v.z, v.w);
+        }
+        return a;
+    }
+    __device__ __forceinline__ M3<float> load(int mu, int s) const {
+        M3<float> a;
+#pragma unroll
+        for (int k = 0; k < kPairs; k++) {
+            const float4 v = __ldg(pair(mu, k) + s);
+            set_elem(a, 2 * k, v.x, v.y);
+            set_elem(a, 2 * k + 1, v.z, v.w);
+        }
+        if (NE == 9) {
+            const float2 v = __ldg(tail(mu) + s);
+            set_elem(a, 8, v.x, v.y);
+        } else {
+            reconstruct_row2(a);
+        }
+        return a;
+    }
+    __device__ __forceinline__ void put_pair(int mu, int k, int s, Cx<float> x, Cx<float> y) const {
+        float4* q = const_cast<float4*>(pair(mu, k)) + s;
+        *q = make_float4(x.re, x.im, y.re, y.im);
+    }
+    __device__ __forceinline__ void store(int mu, int s, const M3<float>& a) const {
+#pragma unroll
+        for (int k = 0; k < kPairs; k++)
+            put_pair(mu, k, s, a.e[(2 * k) / 3][(2 * k) % 3], a.e[(2 * k + 1) / 3][(2 * k + 1) % 3]);
+        if (NE == 9) *(const_cast<float2*>(tail(mu)) + s) = make_float2(a.e[2][2].re, a.e[2][2].im);
+    }
+    __device__ __forceinline__ void store_rows2(int mu, int s, const Rows2<float>& a) const {
+        put_pair(mu, 0, s, a.e[0][0], a.e[0][1]);
+        put_pair(mu, 1, s, a.e[0][2], a.e[1][0]);
+        put_pair(mu, 2, s, a.e[1][1], a.e[1][2]);
+        if (NE == 9) {
+            const Cx<float> r0 = row2_entry(a, 0), r1 = row2_entry(a, 1), r2 = row2_entry(a, 2);
+            put_pair(mu, 3, s, r0, r1);
+            *(const_cast<float2*>(tail(mu)) + s) = make_float2(r2.re, r2.im);
         }
     }
 };
@@ -101,29 +223,53 @@ using FieldF18 = LinkField<float, 9>;
 using FieldF12 = LinkField<float, 6>;
 
 template <class R>
-struct ForceField {
-    R* p;  // [4][8][V]
-    int64_t V;
-    __device__ __forceinline__ Herm8<R> load(int mu, int64_t s) const {
-        const R* b = p + int64_t(mu) * 8 * V + s;
-        Herm8<R> z;
-        z.d0 = b[0];
-        z.d1 = b[V];
-        z.z01 = cx(b[2 * V], b[3 * V]);
-        z.z02 = cx(b[4 * V], b[5 * V]);
-        z.z12 = cx(b[6 * V], b[7 * V]);
+struct ForceField;
+
+template <>
+struct ForceField<double> {
+    void* p;  // 4 double2 planes per mu
+    int V;
+    __device__ __forceinline__ double2* plane(int mu, int k) const {
+        return reinterpret_cast<double2*>(p) + int64_t(mu * 4 + k) * V;
+    }
+    __device__ __forceinline__ Herm8<double> load(int mu, int s) const {
+        const double2 a = plane(mu, 0)[s], b = plane(mu, 1)[s], c = plane(mu, 2)[s], d = plane(mu, 3)[s];
+        Herm8<double> z;
+        z.d0 = a.x;
+        z.d1 = a.y;
+        z.z01 = cx(b.x, b.y);
+        z.z02 = cx(c.x, c.y);
+        z.z12 = cx(d.x, d.y);
         return z;
     }
-    __device__ __forceinline__ void store(int mu, int64_t s, const Herm8<R>& z) const {
-        R* b = p + int64_t(mu) * 8 * V + s;
-        b[0] = z.d0;
-        b[V] = z.d1;
-        b[2 * V] = z.z01.re;
-        b[3 * V] = z.z01.im;
-        b[4 * V] = z.z02.re;
-        b[5 * V] = z.z02.im;
-        b[6 * V] = z.z12.re;
-        b[7 * V] = z.z12.im;
+    __device__ __forceinline__ void store(int mu, int s, const Herm8<double>& z) const {
+        plane(mu, 0)[s] = make_double2(z.d0, z.d1);
+        plane(mu, 1)[s] = make_double2(z.z01.re, z.z01.im);
+        plane(mu, 2)[s] = make_double2(z.z02.re, z.z02.im);
+        plane(mu, 3)[s] = make_double2(z.z12.re, z.z12.im);
+    }
+};
+
+template <>
+struct ForceField<float> {
+    void* p;  // 2 float4 planes per mu
+    int V;
+    __device__ __forceinline__ float4* plane(int mu, int k) const {
+        return reinterpret_cast<float4*>(p) + int64_t(mu * 2 + k) * V;
+    }
+    __device__ __forceinline__ Herm8<float> load(int mu, int s) const {
+        const float4 a = plane(mu, 0)[s], b = plane(mu, 1)[s];
+        Herm8<float> z;
+        z.d0 = a.x;
+        z.d1 = a.y;
+        z.z01 = cx(a.z, a.w);
+        z.z02 = cx(b.x, b.y);
+        z.z12 = cx(b.z, b.w);
+        return z;
+    }
+    __device__ __forceinline__ void store(int mu, int s, const Herm8<float>& z) const {
+        plane(mu, 0)[s] = make_float4(z.d0, z.d1, z.z01.re, z.z01.im);
+        plane(mu, 1)[s] = make_float4(z.z02.re, z.z02.im, z.z12.re, z.z12.im);
     }
 };
 

@@ -10,10 +10,10 @@ namespace ym {
 // One thread per link; the AoS side is read/written 16 bytes at a time.
 // ---------------------------------------------------------------------------
 template <class F>
-__global__ void pack_kernel(const double* __restrict__ aos, F u, int64_t V) {
+__global__ void pack_kernel(const double* __restrict__ aos, F u, int V) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * V) return;
-    const int64_t s = l >> 2;
+    if (l >= 4 * int64_t(V)) return;
+    const int s = int(l >> 2);
     const int mu = int(l & 3);
     const double2* src = reinterpret_cast<const double2*>(aos + l * 18);
     M3<typename F::Real> a;
@@ -26,10 +26,10 @@ __global__ void pack_kernel(const double* __restrict__ aos, F u, int64_t V) {
 }
 
 template <class F>
-__global__ void unpack_kernel(F u, double* __restrict__ aos, int64_t V) {
+__global__ void unpack_kernel(F u, double* __restrict__ aos, int V) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * V) return;
-    const int64_t s = l >> 2;
+    if (l >= 4 * int64_t(V)) return;
+    const int s = int(l >> 2);
     const int mu = int(l & 3);
     const M3<typename F::Real> a = u.load(mu, s);
     double2* dst = reinterpret_cast<double2*>(aos + l * 18);
@@ -41,9 +41,9 @@ cudaError_t launch_pack(int prec, const double* aos, void* u, const Geo& g, cuda
     const int b = 256;
     const unsigned nb = unsigned((4 * g.V + b - 1) / b);
     switch (prec) {
-        case kFP64: pack_kernel<<<nb, b, 0, st>>>(aos, FieldD18{(double2*)u, g.V}, g.V); break;
-        case kFP32_18: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF18{(float2*)u, g.V}, g.V); break;
-        case kFP32_12: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF12{(float2*)u, g.V}, g.V); break;
+        case kFP64: pack_kernel<<<nb, b, 0, st>>>(aos, FieldD18{const_cast<void*>((const void*)u), g.V}, g.V); break;
+        case kFP32_18: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF18{const_cast<void*>((const void*)u), g.V}, g.V); break;
+        case kFP32_12: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF12{const_cast<void*>((const void*)u), g.V}, g.V); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -53,9 +53,9 @@ cudaError_t launch_unpack(int prec, const void* u, double* aos, const Geo& g, cu
     const int b = 256;
     const unsigned nb = unsigned((4 * g.V + b - 1) / b);
     switch (prec) {
-        case kFP64: unpack_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, aos, g.V); break;
-        case kFP32_18: unpack_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, aos, g.V); break;
-        case kFP32_12: unpack_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, aos, g.V); break;
+        case kFP64: unpack_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, aos, g.V); break;
+        case kFP32_18: unpack_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, aos, g.V); break;
+        case kFP32_12: unpack_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, aos, g.V); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -99,10 +99,10 @@ __device__ __forceinline__ double2 gauss2(uint64_t seed, uint32_t config, uint64
 }
 
 template <class F>
-__global__ void init_kernel(F u, int64_t V, int kind, double a, uint64_t seed, uint32_t config) {
+__global__ void init_kernel(F u, int V, int kind, double a, uint64_t seed, uint32_t config) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * V) return;
-    const int64_t s = l >> 2;
+    if (l >= 4 * int64_t(V)) return;
+    const int s = int(l >> 2);
     const int mu = int(l & 3);
     using R = typename F::Real;
     M3<double> m;
@@ -169,9 +169,9 @@ __device__ __forceinline__ void gram_schmidt(M3<double>& m) {
 }
 
 template <class F>
-__global__ void haar_kernel(F u, int64_t V, double frac, uint64_t seed, uint32_t config) {
+__global__ void haar_kernel(F u, int V, double frac, uint64_t seed, uint32_t config) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * V) return;
+    if (l >= 4 * int64_t(V)) return;
     const uint4 o = philox4x32(make_uint4(uint32_t(l), uint32_t(uint64_t(l) >> 32), config, uint32_t(kStreamPick) << 16),
                                make_uint2(uint32_t(seed), uint32_t(seed >> 32)));
     if (!(u53(o.x, o.y) < frac)) return;
@@ -188,7 +188,7 @@ __global__ void haar_kernel(F u, int64_t V, double frac, uint64_t seed, uint32_t
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) r.e[i][j] = cx(R(m.e[i][j].re), R(m.e[i][j].im));
-    u.store(int(l & 3), l >> 2, r);
+    u.store(int(l & 3), int(l >> 2), r);
 }
 
 cudaError_t launch_init_links(int prec, void* u, const Geo& g, int kind, double a, uint64_t seed, uint32_t config,
@@ -196,9 +196,9 @@ cudaError_t launch_init_links(int prec, void* u, const Geo& g, int kind, double 
     const int b = 128;
     const unsigned nb = unsigned((4 * g.V + b - 1) / b);
     switch (prec) {
-        case kFP64: init_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, g.V, kind, a, seed, config); break;
-        case kFP32_18: init_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, g.V, kind, a, seed, config); break;
-        case kFP32_12: init_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, g.V, kind, a, seed, config); break;
+        case kFP64: init_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, g.V, kind, a, seed, config); break;
+        case kFP32_18: init_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, g.V, kind, a, seed, config); break;
+        case kFP32_12: init_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, g.V, kind, a, seed, config); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -209,9 +209,9 @@ cudaError_t launch_haar_mix(int prec, void* u, const Geo& g, double frac, uint64
     const int b = 128;
     const unsigned nb = unsigned((4 * g.V + b - 1) / b);
     switch (prec) {
-        case kFP64: haar_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, g.V, frac, seed, config); break;
-        case kFP32_18: haar_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, g.V, frac, seed, config); break;
-        case kFP32_12: haar_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, g.V, frac, seed, config); break;
+        case kFP64: haar_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, g.V, frac, seed, config); break;
+        case kFP32_18: haar_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, g.V, frac, seed, config); break;
+        case kFP32_12: haar_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, g.V, frac, seed, config); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -222,11 +222,11 @@ cudaError_t launch_haar_mix(int prec, void* u, const Geo& g, double frac, uint64
 // as the reference never does).
 // ---------------------------------------------------------------------------
 template <class F>
-__global__ void reunit_kernel(F u, int64_t V, unsigned long long* deviation) {
+__global__ void reunit_kernel(F u, int V, unsigned long long* deviation) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     double dev = 0.0;
-    if (l < 4 * V) {
-        const int64_t s = l >> 2;
+    if (l < 4 * int64_t(V)) {
+        const int s = int(l >> 2);
         const int mu = int(l & 3);
         const M3<typename F::Real> a = u.load(mu, s);
         M3<double> m;
@@ -260,9 +260,9 @@ cudaError_t launch_reunitarize(int prec, void* u, const Geo& g, unsigned long lo
     const int b = 256;
     const unsigned nb = unsigned((4 * g.V + b - 1) / b);
     switch (prec) {
-        case kFP64: reunit_kernel<<<nb, b, 0, st>>>(FieldD18{(double2*)u, g.V}, g.V, deviation); break;
-        case kFP32_18: reunit_kernel<<<nb, b, 0, st>>>(FieldF18{(float2*)u, g.V}, g.V, deviation); break;
-        case kFP32_12: reunit_kernel<<<nb, b, 0, st>>>(FieldF12{(float2*)u, g.V}, g.V, deviation); break;
+        case kFP64: reunit_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, g.V, deviation); break;
+        case kFP32_18: reunit_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, g.V, deviation); break;
+        case kFP32_12: reunit_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, g.V, deviation); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

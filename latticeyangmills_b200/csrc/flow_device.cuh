@@ -1,0 +1,131 @@
+// Device code of the fused RK3 stage, shared by the single-configuration
+// kernel (flow.cu) and the ensemble kernel (ensemble.cu).
+//
+// Per link (x, mu):
+//   Omega = sum over nu != mu of the upper staple U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
+//           and the lower staple U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
+//           (src/Actions/puregauge.cpp:36-54, same nu order: upper then lower)
+//   D     = (i/2) [U Omega - (U Omega)^+]_traceless     (puregauge.cpp:62-79)
+//   Z     = D                       stage 0   (src/Apps/wilsonflow.cpp:143-144)
+//         = 8/9 D - 17/36 Z_prev    stage 1   (:152-154)
+//         = 3/4 D - Z_prev          stage 2   (:163-165)
+//   U'    = exp(i eps_s Z) U,  eps_s = eps/4, eps, eps   (:147-149, :158-160, :169-171)
+//
+// Stages are Jacobi updates: every Z of a stage is computed from the same
+// field, so links are read from `in` and written to `out` (ping-pong).  Z is
+// written by stages 0 and 1 and read by stages 1 and 2.
+#pragma once
+#include "expsu3.cuh"
+#include "field.cuh"
+
+namespace ym {
+
+// Staples through their first two rows (third row rebuilt as conj(r0 x r1))
+// save 22% of the staple multiply-adds but rebuild a row from rounded rows.
+// In FP64 that costs nothing measurable; in FP32 the rebuilt rows carry a
+// systematic bias that grows linearly with flow time (t^2<E> at t = 4 on 32^4
+// drifts 4e-6 from FP64 against 5e-7 with full products), so the FP32 path
+// forms all three rows.
+template <class R>
+struct kTwoRowStaples {
+    static constexpr bool value = sizeof(R) == 8;
+};
+
+// D_mu(x) = (i/2)[U Omega - (U Omega)^+]_traceless for one link; also returns U_mu(x).
+// Each staple is a product of three SU(3) links; of U Omega only the entries
+// the traceless anti-Hermitian part needs are computed.  mu is warp-uniform and the nu loop is kept rolled: one copy of
+// the staple code serves every direction, which keeps the kernel inside the
+// instruction cache.
+template <class F>
+__device__ __forceinline__ Herm8<typename F::Real> link_force(const F& in, const Geo& g, int s, const int c[4],
+                                                              int mu, M3<typename F::Real>& u) {
+    using R = typename F::Real;
+    M3<R> omega;
+    mzero(omega);
+    const int cmu = g.coord(c, mu);
+    const int s_pm = g.hop_rt(s, cmu, mu, +1);
+#pragma unroll 1
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == mu) continue;
+        const int cnu = g.coord(c, nu);
+        const int s_pn = g.hop_rt(s, cnu, nu, +1);
+        const int s_mn = g.hop_rt(s, cnu, nu, -1);
+        const int s_pm_mn = g.hop_rt(s_mn, cmu, mu, +1);
+        if (kTwoRowStaples<R>::value) {
+            {  // upper staple U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
+                Rows2<R> t, st;
+                {
+                    const Rows2<R> a = in.load_rows2(nu, s_pm);
+                    const M3<R> b = in.load(mu, s_pn);
+                    mmul_rows2<false, true>(a, b, t);
+                }
+                const M3<R> d = in.load(nu, s);
+                mmul_rows2<false, true>(t, d, st);
+                madd_su3_rows2(omega, st);
+            }
+            {  // lower staple U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
+                Rows2<R> t, st;
+                {
+                    const M3<R> a = in.load(nu, s_pm_mn);
+                    const M3<R> b = in.load(mu, s_mn);
+                    mmul_rows2<true, true>(a, b, t);
+                }
+                const M3<R> d = in.load(nu, s_mn);
+                mmul_rows2<false, false>(t, d, st);
+                madd_su3_rows2(omega, st);
+            }
+        } else {
+            {  // upper staple, all three rows
+                M3<R> t;
+                {
+                    const M3<R> a = in.load(nu, s_pm);
+                    const M3<R> b = in.load(mu, s_pn);
+                    mmul<false, true>(a, b, t);
+                }
+                const M3<R> d = in.load(nu, s);
+                mmul_acc<false, true>(t, d, omega);
+            }
+            {  // lower staple, all three rows
+                M3<R> t;
+                {
+                    const M3<R> a = in.load(nu, s_pm_mn);
+                    const M3<R> b = in.load(mu, s_mn);
+                    mmul<true, true>(a, b, t);
+                }
+                const M3<R> d = in.load(nu, s_mn);
+                mmul_acc<false, false>(t, d, omega);
+            }
+        }
+    }
+    u = in.load(mu, s);
+    return force_from_u_omega(u, omega);
+}
+
+// One link through one RK3 stage: generator, RK combination with the stored
+// generator, e^{i eps_s Z} and the update of the link from `in` into `out`.
+template <class F, int STAGE>
+__device__ __forceinline__ void rk_link_update(const F& in, const F& out, const ForceField<typename F::Real>& zf,
+                                               const Geo& g, typename F::Real eps, int s, int mu) {
+    using R = typename F::Real;
+    int c[4];
+    g.coords(s, c);
+    M3<R> u;
+    const Herm8<R> dz = link_force(in, g, s, c, mu, u);
+    Herm8<R> z;
+    if (STAGE == 0) {
+        z = dz;
+        zf.store(mu, s, z);
+    } else if (STAGE == 1) {
+        z = h8_axpby(R(8.0 / 9.0), dz, R(17.0 / 36.0), zf.load(mu, s));
+        zf.store(mu, s, z);
+    } else {
+        z = h8_axpby(R(3.0 / 4.0), dz, R(1.0), zf.load(mu, s));
+    }
+    const Herm8<R> q = h8_scale(eps, z);
+    Rows2<R> e, un;
+    exp_iq_rows2(q, e);
+    mmul_rows2<false, false>(e, u, un);  // e^{iQ} U is in SU(3): two rows suffice
+    out.store_rows2(mu, s, un);
+}
+
+}  // namespace ym

@@ -38,13 +38,13 @@ __device__ __forceinline__ R ah_re_trace_mul(const AH<R>& a, const AH<R>& b) {
 }
 
 template <class F, int MU, int NU>
-__device__ __forceinline__ AH<typename F::Real> clover(const F& u, const Geo& g, int64_t s, const int c[4],
+__device__ __forceinline__ AH<typename F::Real> clover(const F& u, const Geo& g, int s, const int c[4],
                                                        typename F::Real& plaq) {
     using R = typename F::Real;
-    const int64_t s_pm = g.hop(s, c, MU, +1), s_pn = g.hop(s, c, NU, +1);
-    const int64_t s_mm = g.hop(s, c, MU, -1), s_mn = g.hop(s, c, NU, -1);
-    const int64_t s_mm_pn = g.hop(s_mm, c, NU, +1), s_mm_mn = g.hop(s_mm, c, NU, -1);
-    const int64_t s_pm_mn = g.hop(s_pm, c, NU, -1);
+    const int s_pm = g.hop(s, c, MU, +1), s_pn = g.hop(s, c, NU, +1);
+    const int s_mm = g.hop(s, c, MU, -1), s_mn = g.hop(s, c, NU, -1);
+    const int s_mm_pn = g.hop(s_mm, c, NU, +1), s_mm_mn = g.hop(s_mm, c, NU, -1);
+    const int s_pm_mn = g.hop(s_pm, c, NU, -1);
     M3<R> cl, t, w;
     {  // Q1
         mmul<false, false>(u.load(MU, s), u.load(NU, s_pm), t);
@@ -80,7 +80,7 @@ __device__ __forceinline__ AH<typename F::Real> clover(const F& u, const Geo& g,
 }
 
 template <class F>
-__device__ __forceinline__ void site_observables(const F& u, const Geo& g, int64_t s, double& plaq, double& energy,
+__device__ __forceinline__ void site_observables(const F& u, const Geo& g, int s, double& plaq, double& energy,
                                                  double& topc) {
     using R = typename F::Real;
     int c[4];
@@ -143,7 +143,7 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c) {
 
 template <class F>
 __global__ void __launch_bounds__(256) observables_kernel(F u, Geo g, double* partials) {
-    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int s = int(blockIdx.x) * blockDim.x + threadIdx.x;
     double plaq = 0.0, energy = 0.0, topc = 0.0;
     if (s < g.V) site_observables(u, g, s, plaq, energy, topc);
     block_sum3(plaq, energy, topc);
@@ -181,13 +181,13 @@ cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* pa
     const unsigned nb = unsigned(obs_blocks(g, block));
     switch (prec) {
         case kFP64:
-            observables_kernel<<<nb, block, 0, st>>>(FieldD18{(double2*)u, g.V}, g, partials);
+            observables_kernel<<<nb, block, 0, st>>>(FieldD18{const_cast<void*>(u), g.V}, g, partials);
             break;
         case kFP32_18:
-            observables_kernel<<<nb, block, 0, st>>>(FieldF18{(float2*)u, g.V}, g, partials);
+            observables_kernel<<<nb, block, 0, st>>>(FieldF18{const_cast<void*>(u), g.V}, g, partials);
             break;
         case kFP32_12:
-            observables_kernel<<<nb, block, 0, st>>>(FieldF12{(float2*)u, g.V}, g, partials);
+            observables_kernel<<<nb, block, 0, st>>>(FieldF12{const_cast<void*>(u), g.V}, g, partials);
             break;
         default: return cudaErrorInvalidValue;
     }

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "api_util.h"
 #include "kernels.h"
 #include "ymflow.h"
 
@@ -51,27 +52,12 @@ namespace {
 
 thread_local std::string g_create_error;
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int d) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != d) cudaSetDevice(d);
-    }
-    ~DeviceGuard() {
-        int now = -1;
-        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
-    }
-};
-
 int fail(ymflow_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
 }
 
-int cuda_fail(ymflow_ctx* c, cudaError_t e, const char* what) {
-    return fail(c, e == cudaErrorMemoryAllocation ? YMFLOW_ERR_OOM : YMFLOW_ERR_CUDA,
-                std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
-}
+int cuda_fail(ymflow_ctx* c, cudaError_t e, const char* what) { return fail(c, status_of(e), cuda_message(e, what)); }
 
 #define YM_CK(ctx, call, what)                               \
     do {                                                     \
@@ -242,26 +228,17 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
         }
         V *= dims[i];
     }
-    if (V > (int64_t(1) << 31)) {
-        set(YMFLOW_ERR_ARG, "lattice volume above 2^31 sites");
+    if (V >= (int64_t(1) << 31)) {
+        set(YMFLOW_ERR_ARG, "lattice volume must be below 2^31 sites");
         return nullptr;
     }
     if (precision < YMFLOW_FP64 || precision > YMFLOW_FP32_12) {
         set(YMFLOW_ERR_ARG, "unknown precision");
         return nullptr;
     }
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
-        cudaGetLastError();
-        set(YMFLOW_ERR_NODEVICE, "no CUDA device with that index");
-        return nullptr;
-    }
-    int major = 0, minor = 0;
-    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
-    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
-    if (major != 10 || minor != 0) {
-        set(YMFLOW_ERR_NODEVICE, "libymflow is built for sm_100a (B200); device has sm_" + std::to_string(major) +
-                                     std::to_string(minor));
+    std::string why;
+    if (!device_usable(device, &why)) {
+        set(YMFLOW_ERR_NODEVICE, why);
         return nullptr;
     }
     ymflow_ctx* c = new (std::nothrow) ymflow_ctx();
@@ -272,15 +249,8 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     DeviceGuard guard(device);
     c->device = device;
     c->prec = precision;
-    for (int i = 0; i < 4; i++) {
-        c->dims[i] = dims[i];
-        c->geo.n[i] = dims[i];
-    }
-    c->geo.stride[0] = 1;
-    c->geo.stride[1] = dims[0];
-    c->geo.stride[2] = int64_t(dims[0]) * dims[1];
-    c->geo.stride[3] = int64_t(dims[0]) * dims[1] * dims[2];
-    c->geo.V = V;
+    for (int i = 0; i < 4; i++) c->dims[i] = dims[i];
+    c->geo = make_geo(dims);
     int r = YMFLOW_OK;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) r = YMFLOW_ERR_CUDA;
     const size_t ub = size_t(4 * V) * link_bytes(precision);
@@ -520,8 +490,8 @@ int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, 
 int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
     if (!c) return YMFLOW_ERR_ARG;
     switch (key) {
-        case YMFLOW_OPT_BLOCK:
-            if (value < 32 || value > 256 || value % 32) return fail(c, YMFLOW_ERR_ARG, "block must be 32..256, /32");
+        case YMFLOW_OPT_BLOCK:  // four warps (one per direction) per 32 sites
+            if (value != 128 && value != 256) return fail(c, YMFLOW_ERR_ARG, "stage block must be 128 or 256");
             c->block = int(value);
             return YMFLOW_OK;
         case YMFLOW_OPT_OBS_BLOCK:

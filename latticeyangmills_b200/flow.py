@@ -170,6 +170,87 @@ class GluonField:
         return b.value
 
 
+class Ensemble:
+    """Many configurations (any mix of lattice sizes) flowed together on one GPU:
+    one persistent launch per RK3 stage for all of them, steps replayed as a
+    CUDA graph.  The batched form of WilsonFlow::flowConfigurations
+    (src/Apps/wilsonflow.cpp:96-109)."""
+
+    def __init__(self, sizes: Sequence[Sequence[int]], precision: str = "fp32_18", device: int = 0):
+        self.sizes = [tuple(int(v) for v in s) for s in sizes]
+        dims = (ctypes.c_int * (4 * len(self.sizes)))(*[v for s in self.sizes for v in s])
+        st = ctypes.c_int(0)
+        lib = N.load()
+        self._ens = lib.ymflow_ensemble_create(len(self.sizes), dims, N.PRECISIONS[precision], int(device),
+                                               ctypes.byref(st))
+        if not self._ens:
+            raise N.YmflowError(st.value, lib.ymflow_ensemble_last_error(None).decode(errors="replace"))
+        self.precision = precision
+
+    def close(self) -> None:
+        if getattr(self, "_ens", None):
+            N.load().ymflow_ensemble_destroy(self._ens)
+            self._ens = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int) -> None:
+        if status != N.OK:
+            raise N.YmflowError(status, N.load().ymflow_ensemble_last_error(self._ens).decode(errors="replace"))
+
+    def upload(self, conf: int, links: np.ndarray) -> None:
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        if a.size != volume(self.sizes[conf]) * 72:
+            raise ValueError("links must hold 4*V*18 doubles")
+        self._check(N.load().ymflow_ensemble_upload(self._ens, int(conf), a.ctypes.data))
+
+    def download(self, conf: int) -> np.ndarray:
+        n = self.sizes[conf]
+        a = np.empty((n[3], n[2], n[1], n[0], 4, 18), dtype=np.float64)
+        self._check(N.load().ymflow_ensemble_download(self._ens, int(conf), a.ctypes.data))
+        return a
+
+    def init_links(self, conf: int, kind: str = "expiah", a: float = 0.35, seed: int = 1, config: int = 0,
+                   haar_frac: float = 0.0) -> None:
+        k = {"cold": N.FIELD_COLD, "expiah": N.FIELD_EXPIAH}[kind]
+        self._check(N.load().ymflow_ensemble_init_links(self._ens, int(conf), k, float(a), int(seed), int(config),
+                                                        float(haar_frac)))
+
+    def flow(self, eps: float, nsteps: int, measure_every: int = 0, reunit_every: int = 0) -> np.ndarray:
+        """rows x nconf x (step, t, plaq, topc, energy, t2E)."""
+        rows = 1 + sum(1 for s in range(1, nsteps + 1)
+                       if (measure_every > 0 and s % measure_every == 0) or s == nsteps)
+        nc = len(self.sizes)
+        out = (N.Obs * (rows * nc))()
+        n = ctypes.c_int(0)
+        self._check(N.load().ymflow_ensemble_flow(self._ens, float(eps), int(nsteps), int(measure_every),
+                                                  int(reunit_every), out, rows, ctypes.byref(n)))
+        return np.array([out[i].as_tuple() for i in range(n.value * nc)]).reshape(n.value, nc, 6)
+
+    def time_steps(self, eps: float, nsteps: int) -> float:
+        ms = ctypes.c_float(0)
+        self._check(N.load().ymflow_ensemble_time_steps(self._ens, float(eps), int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def autotune(self, eps: float = 0.01):
+        b, g = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(N.load().ymflow_ensemble_autotune(self._ens, float(eps), ctypes.byref(b), ctypes.byref(g)))
+        return b.value, g.value
+
+    def reset_time(self) -> None:
+        self._check(N.load().ymflow_ensemble_reset_time(self._ens))
+
+
 def su3_exp(q: np.ndarray, device: int = 0) -> np.ndarray:
     """e^{iQ} of Hermitian traceless matrices (..., 18) on the GPU: exp(const SU3&)."""
     a = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 18)

@@ -108,6 +108,50 @@ def make_exp_cases():
     print("exp cases", q.shape[0], "nan rows", int(np.isnan(r).any(axis=1).sum()))
 
 
+APP_JSON = {
+    "App": {"type": "FLOW", "params": {"epsilon": 0.01, "tauFinal": 0.1}},
+    "LatticeSize": {"x": 4, "y": 4, "z": 4, "t": 4},
+    "SubLatticeSize": {"x": 4, "y": 4, "z": 4, "t": 4},
+    "Action": {"type": "puregauge", "params": {"beta": 6.0}},
+    "Observables": ["superobs"],
+    "InputDir": "@IN@", "OutputDir": "@OUT@",
+}
+
+
+def app_inputs(indir: Path) -> None:
+    """The FLOW app case's input directory: two 4^4 configurations."""
+    import shutil
+    indir.mkdir(parents=True, exist_ok=True)
+    shutil.copy(OUT / "g4_expiah.bin", indir / "conf0000.bin")
+    shutil.copy(OUT / "g4b_expiah.bin", indir / "conf0001.bin")
+
+
+def make_app_case():
+    """Runs the reference's whole FLOW application (oracle/_ref/lattice_qcd) and
+    keeps its terminal output and output files."""
+    import shutil
+    import subprocess
+    import tempfile
+    yo.write_bin(yo.gen_expiah((4, 4, 4, 4), 0.3, 7), OUT / "g4b_expiah.bin")
+    case = OUT / "app_flow"
+    if case.exists():
+        shutil.rmtree(case)
+    (case / "expected" / "flow").mkdir(parents=True)
+    (case / "input.json").write_text(json.dumps(APP_JSON, indent=1) + "\n")
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        app_inputs(d / "in")
+        text = (case / "input.json").read_text().replace("@IN@", str(d / "in")).replace("@OUT@", str(d / "out"))
+        (d / "run.json").write_text(text)
+        out = subprocess.run([str(yo.HERE / "_ref" / "lattice_qcd"), str(d / "run.json")], check=True,
+                             capture_output=True, text=True).stdout
+        lines = [l for l in out.splitlines(keepends=True) if not l.startswith("Total time taken")]
+        (case / "expected" / "stdout.txt").write_text("".join(lines))
+        for f in ["observables.dat", "flow/conf0000.dat", "flow/conf0001.dat"]:
+            shutil.copy(d / "out" / f, case / "expected" / f)
+    print("app case", len(lines), "terminal lines")
+
+
 def make_deriv_case():
     dims = (4, 4, 4, 4)
     Z = yo.ref_derivative(OUT / "g4_expiah.bin", dims)
@@ -126,3 +170,5 @@ if __name__ == "__main__":
         make_exp_cases()
     if not only or "deriv" in only:
         make_deriv_case()
+    if not only or "app" in only:
+        make_app_case()

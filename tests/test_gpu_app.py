@@ -1,0 +1,53 @@
+"""The drop-in FLOW driver (latticeyangmills_b200/bin/ymflow_flow) against the
+reference's own FLOW application: same JSON, same .bin inputs, and byte-identical
+terminal lines and output files (tests/golden/app_flow, produced by the
+reference binary)."""
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+pytestmark = pytest.mark.gpu
+
+APP = ROOT / "latticeyangmills_b200" / "bin" / "ymflow_flow"
+
+
+def prepare(tmp_path, extra=None):
+    import json
+
+    indir = tmp_path / "in"
+    indir.mkdir()
+    shutil.copy(GOLDEN / "g4_expiah.bin", indir / "conf0000.bin")
+    shutil.copy(GOLDEN / "g4b_expiah.bin", indir / "conf0001.bin")
+    (indir / "notes.txt").write_text("ignored: not a .bin\n")
+    text = (GOLDEN / "app_flow" / "input.json").read_text()
+    text = text.replace("@IN@", str(indir)).replace("@OUT@", str(tmp_path / "out"))
+    cfg = json.loads(text)
+    cfg.update(extra or {})
+    (tmp_path / "run.json").write_text(json.dumps(cfg))
+    return tmp_path / "run.json"
+
+
+def test_flow_app_output_matches_reference_app(tmp_path):
+    run = prepare(tmp_path)
+    res = subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)
+    got = [l for l in res.stdout.splitlines(keepends=True) if not l.startswith("Total time taken")]
+    exp = GOLDEN / "app_flow" / "expected"
+    assert "".join(got) == (exp / "stdout.txt").read_text()
+    for f in ["observables.dat", "flow/conf0000.dat", "flow/conf0001.dat"]:
+        assert (tmp_path / "out" / f).read_bytes() == (exp / f).read_bytes(), f
+    assert (tmp_path / "out" / "flow" / "conf0000.full.dat").exists()
+
+
+def test_flow_app_mixed_precision_rows(tmp_path):
+    run = prepare(tmp_path, {"Precision": "fp32_12", "ReunitEvery": 5})
+    subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)
+    got = (tmp_path / "out" / "flow" / "conf0001.dat").read_text().splitlines()
+    exp = (GOLDEN / "app_flow" / "expected" / "flow" / "conf0001.dat").read_text().splitlines()
+    assert len(got) == len(exp) and got[0] == exp[0]
+    for a, b in zip(got[1:], exp[1:]):
+        va, vb = [float(x) for x in a.split()], [float(x) for x in b.split()]
+        assert va[0] == vb[0]
+        assert abs(va[1] - vb[1]) < 2e-6 and abs(va[3] - vb[3]) < 1e-6 * abs(vb[3]) + 2e-6

@@ -1,0 +1,75 @@
+"""Batched ensemble (one persistent launch per stage for many configurations of
+uneven sizes) against flowing each configuration on its own."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(4, 4, 4, 4), (3, 4, 5, 6), (2, 3, 2, 4), (6, 6, 6, 8), (8, 8, 8, 8)]
+
+
+def single(n, prec, seed, steps, every):
+    from latticeyangmills_b200 import GluonField
+
+    with GluonField(n, prec) as f:
+        f.init_links("expiah", 0.3 + 0.02 * seed, seed)
+        rows = f.flow(0.01, steps, every)
+        return rows, f.download()
+
+
+# the ensemble kernel is a separate compilation of the same link code, so the
+# compiler may contract a few multiply-adds differently: equal to rounding
+LINK_TOL = {"fp64": 1e-13, "fp32_18": 2e-6, "fp32_12": 2e-6}
+OBS_RTOL = {"fp64": 1e-12, "fp32_18": 1e-6, "fp32_12": 1e-6}
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32_18", "fp32_12"])
+def test_ensemble_equals_one_by_one(prec):
+    from latticeyangmills_b200 import Ensemble
+
+    steps, every = 6, 3
+    with Ensemble(SIZES, prec) as ens:
+        for c, n in enumerate(SIZES):
+            ens.init_links(c, "expiah", 0.3 + 0.02 * c, c)
+        rows = ens.flow(0.01, steps, every)
+        for c, n in enumerate(SIZES):
+            want_rows, want_links = single(n, prec, c, steps, every)
+            assert np.abs(ens.download(c) - want_links).max() < LINK_TOL[prec]
+            np.testing.assert_array_equal(rows[:, c, :2], want_rows[:, :2])
+            np.testing.assert_allclose(rows[:, c, [2, 4]], want_rows[:, [2, 4]], rtol=OBS_RTOL[prec])
+
+
+def test_autotune_keeps_state_and_results(oracle):
+    from latticeyangmills_b200 import Ensemble
+
+    with Ensemble(SIZES, "fp32_18") as a, Ensemble(SIZES, "fp32_18") as b:
+        for c in range(len(SIZES)):
+            a.init_links(c, "expiah", 0.35, 10 + c)
+            b.init_links(c, "expiah", 0.35, 10 + c)
+        block, grid = a.autotune()
+        assert block in (128, 256) and grid >= 0
+        ra = a.flow(0.01, 4, 2)
+        rb = b.flow(0.01, 4, 2)
+        np.testing.assert_array_equal(ra, rb)
+        for c in range(len(SIZES)):
+            np.testing.assert_array_equal(a.download(c), b.download(c))
+
+
+def test_ensemble_matches_reference_golden():
+    import json
+
+    from conftest import GOLDEN, case_field, load_case
+    from latticeyangmills_b200 import Ensemble
+
+    names = ["g4_expiah", "g3456_expiah", "g2324_expiah"]
+    cases = [load_case(n) for n in names]
+    with Ensemble([tuple(c["dims"]) for c in cases], "fp64") as ens:
+        for i, c in enumerate(cases):
+            ens.upload(i, case_field(c))
+        rows = ens.flow(0.01, 5, 1)
+    for i, c in enumerate(cases):
+        if c["eps"] != 0.01:
+            continue
+        ref = np.array(c["rows"])[:6]
+        np.testing.assert_allclose(rows[:, i, 2], ref[:, 2], rtol=1e-12)
+        np.testing.assert_allclose(rows[:, i, 4], ref[:, 4], rtol=1e-12)

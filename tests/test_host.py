@@ -1,7 +1,13 @@
 """Host-side logic of the FLOW mirror that needs no GPU: the reference's step
 schedule, the .bin reader and the flow/confNNNN.dat writer."""
+import json
+import shutil
+import subprocess
+
 import numpy as np
 import pytest
+
+from conftest import GOLDEN, ROOT
 
 from latticeyangmills_b200 import WilsonFlow, get_input_list, read_conf, write_conf, write_flow_obs
 
@@ -42,3 +48,31 @@ def test_input_list_sorted_bin_only(tmp_path):
     for name in ["conf0002.bin", "conf0000.bin", "notes.txt", "conf0001.bin"]:
         (tmp_path / name).write_bytes(b"")
     assert [p.split("/")[-1] for p in get_input_list(tmp_path)] == ["conf0000.bin", "conf0001.bin", "conf0002.bin"]
+
+
+APP = ROOT / "latticeyangmills_b200" / "bin" / "ymflow_flow"
+
+
+def _app_input(tmp_path, extra):
+    indir = tmp_path / "in"
+    indir.mkdir()
+    shutil.copy(GOLDEN / "g4_expiah.bin", indir / "conf0000.bin")
+    text = (GOLDEN / "app_flow" / "input.json").read_text()
+    cfg = json.loads(text.replace("@IN@", str(indir)).replace("@OUT@", str(tmp_path / "out")))
+    cfg.update(extra)
+    (tmp_path / "run.json").write_text(json.dumps(cfg))
+    return tmp_path / "run.json"
+
+
+@pytest.mark.parametrize("bad,msg", [
+    ({"App": {"type": "FLOW", "params": {"epsilon": 0.01}}}, "wrong \"FLOW\" app specification"),
+    ({"App": {"type": "PGFG", "params": {}}}, "only \"FLOW\""),
+    ({"Observables": ["wilsonloop"]}, "unknown Observable"),
+    ({"LatticeSize": {"x": 4, "y": 4, "z": 4}}, "wrong LatticeSize specification"),
+    ({"Precision": "fp16"}, "unknown Precision"),
+])
+def test_flow_app_rejects_bad_input(tmp_path, bad, msg):
+    # validation as the reference's JsonInput layer, before any device work
+    run = _app_input(tmp_path, bad)
+    res = subprocess.run([str(APP), str(run)], capture_output=True, text=True)
+    assert res.returncode == 1 and msg in res.stderr
