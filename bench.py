@@ -57,16 +57,23 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(prec: str, dims):
-    """DRAM bytes per stage launch from the committed ncu summary, or None."""
+def profiled_traffic(prec: str, dims, alg_bytes_avg: float):
+    """DRAM bytes of an average stage launch from the committed ncu summary
+    (profiles/), or None.  The summary holds one captured launch (stage 1) with
+    its own algorithmic bytes; its traffic/algorithmic ratio is applied to the
+    average launch of the three stages."""
     name = "rk_stage_%s_%s.md" % ("x".join(str(d) for d in dims), prec)
     p = ROOT / "profiles" / name
     if not p.exists():
         return None
+    vals = {}
     for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
-            return float(line.split(":")[1])
-    return None
+        for key in ("traffic_bytes_per_launch:", "algorithmic_bytes_per_launch:"):
+            if line.startswith(key):
+                vals[key] = float(line.split(":")[1])
+    if len(vals) != 2:
+        return None
+    return vals["traffic_bytes_per_launch:"] / vals["algorithmic_bytes_per_launch:"] * alg_bytes_avg
 
 
 class ClockSampler:
@@ -332,7 +339,7 @@ def our_arm(args, dist: Dist):
     bpl = bytes_per_link_update(prec) * links / 3.0  # algorithmic bytes per stage launch
     avg_launch_s = kernel_ms / 1e3 / (3 * args.steps)
     achieved = bpl / avg_launch_s / 1e9
-    traffic = profiled_traffic(prec, DIMS)
+    traffic = profiled_traffic(prec, DIMS, bpl)
 
     # accuracy of the mixed form against FP64 at t = 4 (400 steps), same seeded field
     accuracy = None
@@ -421,7 +428,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32_12", choices=["fp64", "fp32_18", "fp32_12"])
+    ap.add_argument("--precision", default="fp32_18", choices=["fp64", "fp32_18", "fp32_12"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--skip-ensemble", action="store_true")

@@ -143,7 +143,7 @@ YMFLOW_API int ymflow_reset_time(ymflow_ctx* ctx);
 YMFLOW_API int ymflow_time_steps(ymflow_ctx* ctx, double eps, int nsteps, float* elapsed_ms, float* kernel_ms);
 
 /* Tuning knobs.  key YMFLOW_OPT_BLOCK: threads per block of the stage kernel
- * (128 or 256: four warps, one per direction, per 32 sites); YMFLOW_OPT_OBS_BLOCK:
+ * (128: four warps, one per direction, per 32 sites); YMFLOW_OPT_OBS_BLOCK:
  * threads per block of the observables kernel (32..256, multiple of 32);
  * YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a captured CUDA graph
  * (default), 0 = plain launches. */
@@ -182,8 +182,8 @@ YMFLOW_API int ymflow_ensemble_flow(ymflow_ens* ens, double eps, int nsteps, int
 YMFLOW_API int ymflow_ensemble_reset_time(ymflow_ens* ens);
 /* Device-timed RK3 steps of the whole ensemble (no measurements). */
 YMFLOW_API int ymflow_ensemble_time_steps(ymflow_ens* ens, double eps, int nsteps, float* elapsed_ms);
-/* Times the stage kernel over threads-per-block {128, 256} and persistent grids
- * {one CTA per work item, 1x and 2x the resident CTAs}, keeps the fastest, and
+/* Times the stage kernel over persistent grids {one CTA per work item, 1x and
+ * 2x the resident CTAs} (128 threads per block), keeps the fastest, and
  * caches it for every ensemble of the same sizes and precision in the process.
  * Does not change the flow state. */
 YMFLOW_API int ymflow_ensemble_autotune(ymflow_ens* ens, double eps, int* block, int* grid);

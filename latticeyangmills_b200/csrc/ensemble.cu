@@ -42,8 +42,13 @@ __device__ __forceinline__ int find_conf(const EnsConf* confs, int nconf, int it
     return lo;
 }
 
+template <class F>
+struct EnsMinBlocks {
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : 5;
+};
+
 template <class F, int STAGE>
-__global__ void __launch_bounds__(256) ens_stage_kernel(char* uin, char* uout, char* z,
+__global__ void __launch_bounds__(128, EnsMinBlocks<F>::value) ens_stage_kernel(char* uin, char* uout, char* z,
                                                          const EnsConf* __restrict__ confs, int nconf, int nitems,
                                                          typename F::Real eps) {
     using R = typename F::Real;
@@ -168,7 +173,7 @@ int set_block(ymflow_ens* e, int block) {
     int blk = 0;
     for (EnsConf& c : e->confs) {
         c.blk0 = blk;
-        c.nblk = int((c.g.V + spb - 1) / spb);
+        c.nblk = (c.g.V + spb - 1) / spb;
         blk += c.nblk;
     }
     YE_CK(e, cudaMemcpyAsync(e->confs_dev, e->confs.data(), sizeof(EnsConf) * e->confs.size(),
@@ -348,8 +353,8 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
         C.g = make_geo(d);
         C.uoff = uo;
         C.zoff = zo;
-        uo += int64_t(4) * int64_t(link_bytes(precision)) * V;
-        zo += int64_t(4) * int64_t(force_bytes(precision)) * V;
+        uo += int64_t(4) * int64_t(link_bytes(e->prec)) * V;
+        zo += int64_t(4) * int64_t(force_bytes(e->prec)) * V;
         e->max_v = std::max(e->max_v, V);
         e->signature += std::to_string(d[0]) + "x" + std::to_string(d[1]) + "x" + std::to_string(d[2]) + "x" +
                         std::to_string(d[3]) + ";";
@@ -556,7 +561,7 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
     float best = 1e30f;
     int best_block = e->block, best_grid = e->grid;
-    for (int block : {128, 256}) {
+    for (int block : {128}) {
         int r = set_block(e, block);
         if (r != YMFLOW_OK) return r;
         const int resident = ens_max_resident(e->prec, block);

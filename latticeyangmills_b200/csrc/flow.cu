@@ -16,9 +16,17 @@ __device__ __forceinline__ void link_of_thread(int& s, int& mu) {
     s = int(blockIdx.x) * (blockDim.x >> 2) + ((w >> 2) << 5) + (threadIdx.x & 31);
 }
 
+// Resident 128-thread blocks per SM the stage kernel is compiled for (caps its
+// registers): measured at 32^4 on B200, FP64 is fastest at 128 registers
+// (16 warps) and FP32 at <= 96 (20 warps); more blocks spill.
+template <class F>
+struct StageMinBlocks {
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : 5;
+};
+
 template <class F, int STAGE>
-__global__ void __launch_bounds__(256) rk_stage_kernel(F in, F out, ForceField<typename F::Real> zf, Geo g,
-                                                        typename F::Real eps) {
+__global__ void __launch_bounds__(128, StageMinBlocks<F>::value)
+    rk_stage_kernel(F in, F out, ForceField<typename F::Real> zf, Geo g, typename F::Real eps) {
     int s;
     int mu;
     link_of_thread(s, mu);

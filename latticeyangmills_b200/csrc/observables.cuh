@@ -1,0 +1,164 @@
+// Device code of the observables (plaquette, clover energy, clover charge):
+// per-site values, FP64 block partials and the fixed-order fold.  Shared by
+// observables.cu and any kernel that needs the same reduction.
+#pragma once
+#include "field.cuh"
+#include "su3.cuh"
+
+namespace ym {
+
+// anti-Hermitian traceless G as its imaginary diagonal and upper triangle
+template <class R>
+struct AH {
+    R g0, g1, g2;
+    Cx<R> g01, g02, g12;
+};
+
+template <class R>
+__device__ __forceinline__ R ah_re_trace_mul(const AH<R>& a, const AH<R>& b) {
+    // Re tr(A B) for anti-Hermitian A, B: -sum_i a_ii b_ii - 2 sum_{i<j} Re(A_ij conj(B_ij))
+    R d = a.g0 * b.g0 + a.g1 * b.g1 + a.g2 * b.g2;
+    R o = a.g01.re * b.g01.re + a.g01.im * b.g01.im + a.g02.re * b.g02.re + a.g02.im * b.g02.im +
+          a.g12.re * b.g12.re + a.g12.im * b.g12.im;
+    return -d - R(2) * o;
+}
+
+template <class F, int MU, int NU>
+__device__ __forceinline__ AH<typename F::Real> clover(const F& u, const Geo& g, int s, const int c[4],
+                                                       typename F::Real& plaq) {
+    using R = typename F::Real;
+    const int s_pm = g.hop(s, c, MU, +1), s_pn = g.hop(s, c, NU, +1);
+    const int s_mm = g.hop(s, c, MU, -1), s_mn = g.hop(s, c, NU, -1);
+    const int s_mm_pn = g.hop(s_mm, c, NU, +1), s_mm_mn = g.hop(s_mm, c, NU, -1);
+    const int s_pm_mn = g.hop(s_pm, c, NU, -1);
+    M3<R> cl, t, w;
+    {  // Q1
+        mmul<false, false>(u.load(MU, s), u.load(NU, s_pm), t);
+        mmul<false, true>(t, u.load(MU, s_pn), w);
+        mmul<false, true>(w, u.load(NU, s), cl);
+        plaq = re_trace(cl);
+    }
+    {  // Q2
+        mmul<false, true>(u.load(NU, s), u.load(MU, s_mm_pn), t);
+        mmul<false, true>(t, u.load(NU, s_mm), w);
+        mmul_acc<false, false>(w, u.load(MU, s_mm), cl);
+    }
+    {  // Q3
+        mmul<true, true>(u.load(MU, s_mm), u.load(NU, s_mm_mn), t);
+        mmul<false, false>(t, u.load(MU, s_mm_mn), w);
+        mmul_acc<false, false>(w, u.load(NU, s_mn), cl);
+    }
+    {  // Q4
+        mmul<true, false>(u.load(NU, s_mn), u.load(MU, s_mn), t);
+        mmul<false, false>(t, u.load(NU, s_pm_mn), w);
+        mmul_acc<false, true>(w, u.load(MU, s), cl);
+    }
+    AH<R> G;
+    const R i0 = R(2) * cl.e[0][0].im, i1 = R(2) * cl.e[1][1].im, i2 = R(2) * cl.e[2][2].im;
+    const R m = (i0 + i1 + i2) * R(1.0 / 3.0);
+    G.g0 = i0 - m;
+    G.g1 = i1 - m;
+    G.g2 = i2 - m;
+    G.g01 = cx(cl.e[0][1].re - cl.e[1][0].re, cl.e[0][1].im + cl.e[1][0].im);
+    G.g02 = cx(cl.e[0][2].re - cl.e[2][0].re, cl.e[0][2].im + cl.e[2][0].im);
+    G.g12 = cx(cl.e[1][2].re - cl.e[2][1].re, cl.e[1][2].im + cl.e[2][1].im);
+    return G;
+}
+
+template <class F>
+__device__ __forceinline__ void site_observables(const F& u, const Geo& g, int s, double& plaq, double& energy,
+                                                 double& topc) {
+    using R = typename F::Real;
+    int c[4];
+    g.coords(s, c);
+    R p;
+    AH<R> a, b;
+    a = clover<F, 0, 1>(u, g, s, c, p);
+    plaq += double(p);
+    energy += double(ah_re_trace_mul(a, a));
+    b = clover<F, 2, 3>(u, g, s, c, p);
+    plaq += double(p);
+    energy += double(ah_re_trace_mul(b, b));
+    double q = double(ah_re_trace_mul(a, b));
+    a = clover<F, 0, 2>(u, g, s, c, p);
+    plaq += double(p);
+    energy += double(ah_re_trace_mul(a, a));
+    b = clover<F, 1, 3>(u, g, s, c, p);
+    plaq += double(p);
+    energy += double(ah_re_trace_mul(b, b));
+    q -= double(ah_re_trace_mul(a, b));  // Re tr(G02 G13^+) = -Re tr(G02 G13)
+    a = clover<F, 0, 3>(u, g, s, c, p);
+    plaq += double(p);
+    energy += double(ah_re_trace_mul(a, a));
+    b = clover<F, 1, 2>(u, g, s, c, p);
+    plaq += double(p);
+    energy += double(ah_re_trace_mul(b, b));
+    q += double(ah_re_trace_mul(a, b));
+    topc -= q;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sums three values over the block; thread 0 gets the totals.
+__device__ __forceinline__ void block_sum3(double& a, double& b, double& c) {
+    __shared__ double sh[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    if (lane == 0) {
+        sh[0][wid] = a;
+        sh[1][wid] = b;
+        sh[2][wid] = c;
+    }
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    if (wid == 0) {
+        a = lane < nw ? sh[0][lane] : 0.0;
+        b = lane < nw ? sh[1][lane] : 0.0;
+        c = lane < nw ? sh[2][lane] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        c = warp_sum(c);
+    }
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) observables_kernel(F u, Geo g, double* partials) {
+    const int s = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    double plaq = 0.0, energy = 0.0, topc = 0.0;
+    if (s < g.V) site_observables(u, g, s, plaq, energy, topc);
+    block_sum3(plaq, energy, topc);
+    if (threadIdx.x == 0) {
+        partials[3 * blockIdx.x + 0] = plaq;
+        partials[3 * blockIdx.x + 1] = energy;
+        partials[3 * blockIdx.x + 2] = topc;
+    }
+}
+
+// One block of 1024 threads: thread i folds partials i, i+1024, ... in order,
+// then the block tree.  Output (plaq, topc, energy, nonfinite flag).
+__global__ void __launch_bounds__(1024) obs_finalize_kernel(const double* partials, int nblocks, double inv_18v,
+                                                            double* out) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+        a += partials[3 * i + 0];
+        b += partials[3 * i + 1];
+        c += partials[3 * i + 2];
+    }
+    block_sum3(a, b, c);
+    if (threadIdx.x == 0) {
+        const double plaq = a * inv_18v;
+        const double topc = c / (256.0 * 3.14159265358979323846 * 3.14159265358979323846);
+        out[0] = plaq;
+        out[1] = topc;
+        out[2] = b;
+        out[3] = (isfinite(plaq) && isfinite(topc) && isfinite(b)) ? 0.0 : 1.0;
+    }
+}
+
+}  // namespace ym

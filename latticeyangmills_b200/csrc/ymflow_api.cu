@@ -253,8 +253,8 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     c->geo = make_geo(dims);
     int r = YMFLOW_OK;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) r = YMFLOW_ERR_CUDA;
-    const size_t ub = size_t(4 * V) * link_bytes(precision);
-    const size_t zb = size_t(4 * V) * force_bytes(precision);
+    const size_t ub = size_t(4 * V) * link_bytes(c->prec);
+    const size_t zb = size_t(4 * V) * force_bytes(c->prec);
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[0], ub, "link buffer 0");
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[1], ub, "link buffer 1");
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->z, zb, "force buffer");
@@ -491,7 +491,7 @@ int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
     if (!c) return YMFLOW_ERR_ARG;
     switch (key) {
         case YMFLOW_OPT_BLOCK:  // four warps (one per direction) per 32 sites
-            if (value != 128 && value != 256) return fail(c, YMFLOW_ERR_ARG, "stage block must be 128 or 256");
+            if (value != 128) return fail(c, YMFLOW_ERR_ARG, "stage block must be 128 (compiled launch bounds)");
             c->block = int(value);
             return YMFLOW_OK;
         case YMFLOW_OPT_OBS_BLOCK:

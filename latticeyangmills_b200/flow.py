@@ -164,6 +164,11 @@ class GluonField:
     def set_option(self, key: int, value: int) -> None:
         self._check(N.load().ymflow_set_option(self.ctx, int(key), int(value)))
 
+    def get_option(self, key: int) -> int:
+        v = ctypes.c_int64(0)
+        self._check(N.load().ymflow_get_option(self.ctx, int(key), ctypes.byref(v)))
+        return v.value
+
     def device_bytes(self) -> int:
         b = ctypes.c_int64(0)
         self._check(N.load().ymflow_device_bytes(self.ctx, ctypes.byref(b)))

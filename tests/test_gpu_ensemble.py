@@ -19,7 +19,7 @@ def single(n, prec, seed, steps, every):
 
 # the ensemble kernel is a separate compilation of the same link code, so the
 # compiler may contract a few multiply-adds differently: equal to rounding
-LINK_TOL = {"fp64": 1e-13, "fp32_18": 2e-6, "fp32_12": 2e-6}
+LINK_TOL = {"fp64": 1e-13, "fp32_18": 1e-5, "fp32_12": 1e-5}
 OBS_RTOL = {"fp64": 1e-12, "fp32_18": 1e-6, "fp32_12": 1e-6}
 
 
@@ -47,7 +47,7 @@ def test_autotune_keeps_state_and_results(oracle):
             a.init_links(c, "expiah", 0.35, 10 + c)
             b.init_links(c, "expiah", 0.35, 10 + c)
         block, grid = a.autotune()
-        assert block in (128, 256) and grid >= 0
+        assert block == 128 and grid >= 0
         ra = a.flow(0.01, 4, 2)
         rb = b.flow(0.01, 4, 2)
         np.testing.assert_array_equal(ra, rb)

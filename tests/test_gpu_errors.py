@@ -56,7 +56,7 @@ def test_bad_options_rejected():
     from latticeyangmills_b200 import _native as N
 
     with GluonField((4, 4, 4, 4)) as f:
-        for key, val in [(N.OPT_BLOCK, 64), (N.OPT_BLOCK, 1024), (N.OPT_OBS_BLOCK, 48), (99, 1)]:
+        for key, val in [(N.OPT_BLOCK, 64), (N.OPT_BLOCK, 256), (N.OPT_OBS_BLOCK, 48), (99, 1)]:
             with pytest.raises(YmflowError):
                 f.set_option(key, val)
 

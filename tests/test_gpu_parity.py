@@ -111,7 +111,7 @@ def test_graph_and_block_size_do_not_change_results():
     case = load_case("g3456_expiah")
     U = case_field(case)
     outs = []
-    for graph, block, obs_block in [(1, 128, 128), (0, 128, 64), (1, 256, 256), (0, 256, 32)]:
+    for graph, block, obs_block in [(1, 128, 128), (0, 128, 64), (1, 128, 256), (0, 128, 32)]:
         with GluonField(tuple(case["dims"]), "fp64") as f:
             f.set_option(N.OPT_GRAPH, graph)
             f.set_option(N.OPT_BLOCK, block)
