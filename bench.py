@@ -147,8 +147,9 @@ class Dist:
             import torch.distributed as dist
 
             self.torch = torch
-            torch.cuda.set_device(self.local)
             backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
             dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.dist = dist
             self.dev = torch.device("cuda", self.local) if backend == "nccl" else torch.device("cpu")

@@ -20,17 +20,6 @@
 
 namespace ym {
 
-// Staples through their first two rows (third row rebuilt as conj(r0 x r1))
-// save 22% of the staple multiply-adds but rebuild a row from rounded rows.
-// In FP64 that costs nothing measurable; in FP32 the rebuilt rows carry a
-// systematic bias that grows linearly with flow time (t^2<E> at t = 4 on 32^4
-// drifts 4e-6 from FP64 against 5e-7 with full products), so the FP32 path
-// forms all three rows.
-template <class R>
-struct kTwoRowStaples {
-    static constexpr bool value = sizeof(R) == 8;
-};
-
 // D_mu(x) = (i/2)[U Omega - (U Omega)^+]_traceless for one link; also returns U_mu(x).
 // Each staple is a product of three SU(3) links; of U Omega only the entries
 // the traceless anti-Hermitian part needs are computed.  mu is warp-uniform and the nu loop is kept rolled: one copy of

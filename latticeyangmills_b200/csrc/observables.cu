@@ -22,6 +22,27 @@
 
 namespace ym {
 
+// One block of 1024 threads: thread i folds partials i, i+1024, ... in order,
+// then the block tree.  Output (plaq, topc, energy, nonfinite flag).
+__global__ void __launch_bounds__(1024) obs_finalize_kernel(const double* partials, int nblocks, double inv_18v,
+                                                            double* out) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+        a += partials[3 * i + 0];
+        b += partials[3 * i + 1];
+        c += partials[3 * i + 2];
+    }
+    block_sum3(a, b, c);
+    if (threadIdx.x == 0) {
+        const double plaq = a * inv_18v;
+        const double topc = c / (256.0 * 3.14159265358979323846 * 3.14159265358979323846);
+        out[0] = plaq;
+        out[1] = topc;
+        out[2] = b;
+        out[3] = (isfinite(plaq) && isfinite(topc) && isfinite(b)) ? 0.0 : 1.0;
+    }
+}
+
 int obs_blocks(const Geo& g, int block) { return int((g.V + block - 1) / block); }
 
 cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* partials, int block, cudaStream_t st) {

@@ -23,36 +23,8 @@ __device__ __forceinline__ R ah_re_trace_mul(const AH<R>& a, const AH<R>& b) {
     return -d - R(2) * o;
 }
 
-template <class F, int MU, int NU>
-__device__ __forceinline__ AH<typename F::Real> clover(const F& u, const Geo& g, int s, const int c[4],
-                                                       typename F::Real& plaq) {
-    using R = typename F::Real;
-    const int s_pm = g.hop(s, c, MU, +1), s_pn = g.hop(s, c, NU, +1);
-    const int s_mm = g.hop(s, c, MU, -1), s_mn = g.hop(s, c, NU, -1);
-    const int s_mm_pn = g.hop(s_mm, c, NU, +1), s_mm_mn = g.hop(s_mm, c, NU, -1);
-    const int s_pm_mn = g.hop(s_pm, c, NU, -1);
-    M3<R> cl, t, w;
-    {  // Q1
-        mmul<false, false>(u.load(MU, s), u.load(NU, s_pm), t);
-        mmul<false, true>(t, u.load(MU, s_pn), w);
-        mmul<false, true>(w, u.load(NU, s), cl);
-        plaq = re_trace(cl);
-    }
-    {  // Q2
-        mmul<false, true>(u.load(NU, s), u.load(MU, s_mm_pn), t);
-        mmul<false, true>(t, u.load(NU, s_mm), w);
-        mmul_acc<false, false>(w, u.load(MU, s_mm), cl);
-    }
-    {  // Q3
-        mmul<true, true>(u.load(MU, s_mm), u.load(NU, s_mm_mn), t);
-        mmul<false, false>(t, u.load(MU, s_mm_mn), w);
-        mmul_acc<false, false>(w, u.load(NU, s_mn), cl);
-    }
-    {  // Q4
-        mmul<true, false>(u.load(NU, s_mn), u.load(MU, s_mn), t);
-        mmul<false, false>(t, u.load(NU, s_pm_mn), w);
-        mmul_acc<false, true>(w, u.load(MU, s), cl);
-    }
+template <class R>
+__device__ __forceinline__ AH<R> ah_of_clover(const M3<R>& cl) {
     AH<R> G;
     const R i0 = R(2) * cl.e[0][0].im, i1 = R(2) * cl.e[1][1].im, i2 = R(2) * cl.e[2][2].im;
     const R m = (i0 + i1 + i2) * R(1.0 / 3.0);
@@ -65,35 +37,98 @@ __device__ __forceinline__ AH<typename F::Real> clover(const F& u, const Geo& g,
     return G;
 }
 
+// G_{mu nu}(x) and Re tr Q1.  In FP64 each leaf (a product of four SU(3)
+// links) is formed through its first two rows with the third rebuilt
+// (exact to FP64 rounding, and it keeps the kernel within its registers); the
+// FP32 forms multiply all three rows (see kTwoRowStaples in su3.cuh).
+template <class F>
+__device__ __forceinline__ AH<typename F::Real> clover(const F& u, const Geo& g, int s, const int c[4], int MU, int NU,
+                                                       typename F::Real& plaq) {
+    using R = typename F::Real;
+    const int cmu = g.coord(c, MU), cnu = g.coord(c, NU);
+    const int s_pm = g.hop_rt(s, cmu, MU, +1), s_pn = g.hop_rt(s, cnu, NU, +1);
+    const int s_mm = g.hop_rt(s, cmu, MU, -1), s_mn = g.hop_rt(s, cnu, NU, -1);
+    const int s_mm_pn = g.hop_rt(s_mm, cnu, NU, +1), s_mm_mn = g.hop_rt(s_mm, cnu, NU, -1);
+    const int s_pm_mn = g.hop_rt(s_pm, cnu, NU, -1);
+    M3<R> cl;
+    if (kTwoRowStaples<R>::value) {
+        Rows2<R> t, w, l;
+        {  // Q1
+            mmul_rows2<false, false>(u.load_rows2(MU, s), u.load(NU, s_pm), t);
+            mmul_rows2<false, true>(t, u.load(MU, s_pn), w);
+            mmul_rows2<false, true>(w, u.load(NU, s), l);
+            full_from_rows2(l, cl);
+            plaq = re_trace(cl);
+        }
+        {  // Q2
+            mmul_rows2<false, true>(u.load_rows2(NU, s), u.load(MU, s_mm_pn), t);
+            mmul_rows2<false, true>(t, u.load(NU, s_mm), w);
+            mmul_rows2<false, false>(w, u.load(MU, s_mm), l);
+            madd_su3_rows2(cl, l);
+        }
+        {  // Q3
+            mmul_rows2<true, true>(u.load(MU, s_mm), u.load(NU, s_mm_mn), t);
+            mmul_rows2<false, false>(t, u.load(MU, s_mm_mn), w);
+            mmul_rows2<false, false>(w, u.load(NU, s_mn), l);
+            madd_su3_rows2(cl, l);
+        }
+        {  // Q4
+            mmul_rows2<true, false>(u.load(NU, s_mn), u.load(MU, s_mn), t);
+            mmul_rows2<false, false>(t, u.load(NU, s_pm_mn), w);
+            mmul_rows2<false, true>(w, u.load(MU, s), l);
+            madd_su3_rows2(cl, l);
+        }
+    } else {
+        M3<R> t, w;
+        {  // Q1
+            mmul<false, false>(u.load(MU, s), u.load(NU, s_pm), t);
+            mmul<false, true>(t, u.load(MU, s_pn), w);
+            mmul<false, true>(w, u.load(NU, s), cl);
+            plaq = re_trace(cl);
+        }
+        {  // Q2
+            mmul<false, true>(u.load(NU, s), u.load(MU, s_mm_pn), t);
+            mmul<false, true>(t, u.load(NU, s_mm), w);
+            mmul_acc<false, false>(w, u.load(MU, s_mm), cl);
+        }
+        {  // Q3
+            mmul<true, true>(u.load(MU, s_mm), u.load(NU, s_mm_mn), t);
+            mmul<false, false>(t, u.load(MU, s_mm_mn), w);
+            mmul_acc<false, false>(w, u.load(NU, s_mn), cl);
+        }
+        {  // Q4
+            mmul<true, false>(u.load(NU, s_mn), u.load(MU, s_mn), t);
+            mmul<false, false>(t, u.load(NU, s_pm_mn), w);
+            mmul_acc<false, true>(w, u.load(MU, s), cl);
+        }
+    }
+    return ah_of_clover(cl);
+}
+
+// The planes in the pairs (01,23), (02,13), (03,12); the pair loop is kept
+// rolled so one copy of the clover code serves all six planes.
 template <class F>
 __device__ __forceinline__ void site_observables(const F& u, const Geo& g, int s, double& plaq, double& energy,
                                                  double& topc) {
     using R = typename F::Real;
     int c[4];
     g.coords(s, c);
-    R p;
-    AH<R> a, b;
-    a = clover<F, 0, 1>(u, g, s, c, p);
-    plaq += double(p);
-    energy += double(ah_re_trace_mul(a, a));
-    b = clover<F, 2, 3>(u, g, s, c, p);
-    plaq += double(p);
-    energy += double(ah_re_trace_mul(b, b));
-    double q = double(ah_re_trace_mul(a, b));
-    a = clover<F, 0, 2>(u, g, s, c, p);
-    plaq += double(p);
-    energy += double(ah_re_trace_mul(a, a));
-    b = clover<F, 1, 3>(u, g, s, c, p);
-    plaq += double(p);
-    energy += double(ah_re_trace_mul(b, b));
-    q -= double(ah_re_trace_mul(a, b));  // Re tr(G02 G13^+) = -Re tr(G02 G13)
-    a = clover<F, 0, 3>(u, g, s, c, p);
-    plaq += double(p);
-    energy += double(ah_re_trace_mul(a, a));
-    b = clover<F, 1, 2>(u, g, s, c, p);
-    plaq += double(p);
-    energy += double(ah_re_trace_mul(b, b));
-    q += double(ah_re_trace_mul(a, b));
+    double q = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) {
+        const int mu_b = k == 0 ? 2 : 1;
+        const int nu_a = k + 1, nu_b = k == 0 ? 3 : (k == 1 ? 3 : 2);
+        R p;
+        const AH<R> a = clover(u, g, s, c, 0, nu_a, p);
+        plaq += double(p);
+        energy += double(ah_re_trace_mul(a, a));
+        const AH<R> b = clover(u, g, s, c, mu_b, nu_b, p);
+        plaq += double(p);
+        energy += double(ah_re_trace_mul(b, b));
+        // Re tr(G01 G23), Re tr(G02 G13^+) = -Re tr(G02 G13), Re tr(G03 G12)
+        const double t = double(ah_re_trace_mul(a, b));
+        q += k == 1 ? -t : t;
+    }
     topc -= q;
 }
 
@@ -137,27 +172,6 @@ __global__ void __launch_bounds__(256) observables_kernel(F u, Geo g, double* pa
         partials[3 * blockIdx.x + 0] = plaq;
         partials[3 * blockIdx.x + 1] = energy;
         partials[3 * blockIdx.x + 2] = topc;
-    }
-}
-
-// One block of 1024 threads: thread i folds partials i, i+1024, ... in order,
-// then the block tree.  Output (plaq, topc, energy, nonfinite flag).
-__global__ void __launch_bounds__(1024) obs_finalize_kernel(const double* partials, int nblocks, double inv_18v,
-                                                            double* out) {
-    double a = 0.0, b = 0.0, c = 0.0;
-    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
-        a += partials[3 * i + 0];
-        b += partials[3 * i + 1];
-        c += partials[3 * i + 2];
-    }
-    block_sum3(a, b, c);
-    if (threadIdx.x == 0) {
-        const double plaq = a * inv_18v;
-        const double topc = c / (256.0 * 3.14159265358979323846 * 3.14159265358979323846);
-        out[0] = plaq;
-        out[1] = topc;
-        out[2] = b;
-        out[3] = (isfinite(plaq) && isfinite(topc) && isfinite(b)) ? 0.0 : 1.0;
     }
 }
 

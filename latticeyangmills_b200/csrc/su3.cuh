@@ -211,6 +211,17 @@ __device__ __forceinline__ void full_from_rows2(const Rows2<R>& a, M3<R>& m) {
     for (int k = 0; k < 3; k++) m.e[2][k] = row2_entry(a, k);
 }
 
+// Products of SU(3) links through their first two rows (third row rebuilt as conj(r0 x r1))
+// save 22% of the staple multiply-adds but rebuild a row from rounded rows.
+// In FP64 that costs nothing measurable; in FP32 the rebuilt rows carry a
+// systematic bias that grows linearly with flow time (t^2<E> at t = 4 on 32^4
+// drifts 4e-6 from FP64 against 5e-7 with full products), so the FP32 path
+// forms all three rows.
+template <class R>
+struct kTwoRowStaples {
+    static constexpr bool value = sizeof(R) == 8;
+};
+
 // Entry (i,j) of u * w (full matrices).
 template <class R>
 __device__ __forceinline__ Cx<R> mul_entry(const M3<R>& u, const M3<R>& w, int i, int j) {
