@@ -160,6 +160,28 @@ YMFLOW_API int ymflow_host_free(void* ptr);
 /* Device bytes held by the context (links x2, force, staging, scratch). */
 YMFLOW_API int ymflow_device_bytes(const ymflow_ctx* ctx, int64_t* bytes);
 
+/* ---- allocation-free observables ----------------------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that cannot
+ * call cudaMalloc where they measure, e.g. a host application that reserved the
+ * whole device for its own memory pool, or a latency-critical loop that cannot
+ * take the implicit synchronisation of an allocation.
+ *
+ * Computes plaq, topc and energy (as ymflow_observables) of a configuration the
+ * caller holds in DEVICE memory in the .bin layout (4*V*18 doubles, FP64) and
+ * writes out_device[0..3] = plaq, topc, energy, non-finite flag (0 or 1), in
+ * device memory, asynchronously on `stream` (a cudaStream_t; NULL = default
+ * stream) of the current device.  Allocates nothing: its scratch is a fixed
+ * 1.5 MB device array inside the library (held by every GPU that loads it),
+ * which limits the lattice to YMFLOW_NOALLOC_MAX_SITES sites; larger lattices
+ * return YMFLOW_ERR_CAPACITY.  The first call on a device looks the array's
+ * device address up once and should come before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race and must be ordered by
+ * the caller.  Returns YMFLOW_ERR_ARG, YMFLOW_ERR_CAPACITY, YMFLOW_ERR_NODEVICE
+ * or YMFLOW_ERR_CUDA (launch failure) on error. */
+#define YMFLOW_NOALLOC_MAX_SITES 8388608
+YMFLOW_API int ymflow_observables_noalloc(const double* links_aos_device, const int dims[4], double* out_device,
+                                          void* stream);
+
 /* ---- batched ensemble --------------------------------------------------------------
  * Many configurations, of any mix of lattice sizes, flowed together: every RK3
  * stage of every configuration is one persistent launch over a work list of

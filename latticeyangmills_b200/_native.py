@@ -22,6 +22,7 @@ ERR_UNITARITY = -5
 ERR_CAPACITY = -6
 ERR_STATE = -7
 ERR_NODEVICE = -8
+NOALLOC_MAX_SITES = 8388608  # YMFLOW_NOALLOC_MAX_SITES
 
 FP64, FP32_18, FP32_12 = 0, 1, 2
 PRECISIONS = {"fp64": FP64, "fp32_18": FP32_18, "fp32_12": FP32_12}
@@ -37,7 +38,7 @@ EXPORTS = (
     "ymflow_ensemble_create", "ymflow_ensemble_destroy", "ymflow_ensemble_last_error",
     "ymflow_ensemble_upload", "ymflow_ensemble_download", "ymflow_ensemble_init_links",
     "ymflow_ensemble_flow", "ymflow_ensemble_reset_time", "ymflow_ensemble_time_steps",
-    "ymflow_ensemble_autotune",
+    "ymflow_ensemble_autotune", "ymflow_observables_noalloc",
 )
 NON_INT = ("ymflow_version", "ymflow_create", "ymflow_destroy", "ymflow_last_error", "ymflow_ensemble_create",
            "ymflow_ensemble_destroy", "ymflow_ensemble_last_error")
@@ -117,6 +118,7 @@ def load():
     l.ymflow_ensemble_reset_time.argtypes = [vp]
     l.ymflow_ensemble_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     l.ymflow_ensemble_autotune.argtypes = [vp, ctypes.c_double, IP, IP]
+    l.ymflow_observables_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_int), vp, vp]
     for name in EXPORTS:
         if name not in NON_INT:
             getattr(l, name).restype = ctypes.c_int
