@@ -287,6 +287,51 @@ def ensemble_measure(prec: str, steps: int, dev: int):
             "speedup_vs_one_by_one": one_ms / ms, "autotuned": {"block": block, "grid": grid}}
 
 
+def workload_run(args, dev: int):
+    """The other configurations of the benchmark set, each flowed in every precision
+    from the same seeded field, with each observable's error against FP64:
+      16x32: 16^3 x 32, a = 0.35, eps 0.01 to t = 2, observables every 10 steps
+      64:    64^4, a = 0.35 plus 5 % Haar-random links, eps 0.02 to t = 6,
+             observables every 5 steps (about 24 GB in FP64)."""
+    import time
+
+    import numpy as np
+
+    from latticeyangmills_b200 import GluonField
+
+    if args.workload == "16x32":
+        dims, a, haar, eps, nsteps, every = (16, 16, 16, 32), A, 0.0, 0.01, 200, 10
+    else:
+        dims, a, haar, eps, nsteps, every = (64, 64, 64, 64), A, 0.05, 0.02, 300, 5
+    links = 4 * dims[0] * dims[1] * dims[2] * dims[3]
+    res = {}
+    for p in ["fp64", "fp32_18", "fp32_12"]:
+        f = GluonField(dims, p, device=dev)
+        f.init_links("expiah", a, SEED, 0, haar)
+        t0 = time.perf_counter()
+        rows = f.flow(eps, nsteps, every, reunit_every=10 if p != "fp64" else 0)
+        wall = time.perf_counter() - t0
+        f.init_links("expiah", a, SEED, 0, haar)
+        f.time_steps(eps, 3)
+        ms, _ = f.time_steps(eps, 20)
+        f.close()
+        res[p] = (rows, links * 20 / (ms / 1e3), wall)
+    r64 = res["fp64"][0]
+    out = {"workload": args.workload, "lattice": list(dims), "eps": eps, "steps": nsteps, "measure_every": every,
+           "haar_fraction": haar, "t_final": float(r64[-1, 1]), "t2E_fp64_final": float(r64[-1, 5]),
+           "Q_fp64_final": float(r64[-1, 3])}
+    for p in ["fp64", "fp32_18", "fp32_12"]:
+        rows, lups, wall = res[p]
+        d = {"link_updates_per_s": lups, "flow_wall_s_with_measurements": wall}
+        if p != "fp64":
+            rel = np.abs(rows[1:, 5] - r64[1:, 5]) / np.abs(r64[1:, 5])
+            d.update({"max_rel_err_t2E": float(rel.max()), "rel_err_t2E_final": float(rel[-1]),
+                      "max_abs_err_Q": float(np.abs(rows[:, 3] - r64[:, 3]).max()),
+                      "max_abs_err_plaq": float(np.abs(rows[:, 2] - r64[:, 2]).max())})
+        out[p] = d
+    print(json.dumps(out))
+
+
 def our_arm(args, dist: Dist):
     import ctypes
 
@@ -434,6 +479,9 @@ def main():
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--lattice", type=int, default=32, help="L of the L^4 lattice (profiling of smaller cases)")
+    ap.add_argument("--workload", default="32", choices=["32", "16x32", "64"],
+                    help="32: the headline 32^4 benchmark; 16x32 / 64: accuracy and throughput of the other "
+                         "configurations against FP64")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps of one precision (for ncu captures)")
     args = ap.parse_args()
@@ -445,6 +493,9 @@ def main():
         # CPU-only: under torchrun rank 0 runs and prints, the other ranks exit at once
         if int(os.environ.get("RANK", "0")) == 0:
             reference_arm(args)
+        return
+    if args.workload != "32":
+        workload_run(args, int(os.environ.get("LOCAL_RANK", "0")))
         return
     dist = Dist(args.gpus)
     try:
