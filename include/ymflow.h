@@ -54,6 +54,8 @@ extern "C" {
 /* ---- seeded synthetic fields (ymflow_init_links) ------------------------------------ */
 #define YMFLOW_FIELD_COLD 0    /* every link the identity */
 #define YMFLOW_FIELD_EXPIAH 1  /* U = e^{i a H}, H traceless Hermitian, iid N(0,1) reals */
+#define YMFLOW_FIELD_HOT 2     /* (ymflow_generate_metropolis start) Haar-random links */
+#define YMFLOW_FIELD_CURRENT 3 /* (ymflow_generate_metropolis start) continue from the current links */
 
 typedef struct ymflow_ctx ymflow_ctx;
 
@@ -101,6 +103,22 @@ YMFLOW_API int ymflow_download(ymflow_ctx* ctx, double* links_aos);
  * EXPIAH (scale a); then, if haar_frac > 0, replace that fraction of links
  * (seeded Bernoulli) by Haar-random SU(3).  Same recipe as the test fixtures. */
 YMFLOW_API int ymflow_init_links(ymflow_ctx* ctx, int kind, double a, uint64_t seed, uint32_t config, double haar_frac);
+
+/* Generate a configuration by Metropolis updates of the Wilson action at
+ * `beta`: `sweeps` sweeps, each a checkerboard over (mu, site parity), `hits`
+ * proposals X U per link with X a product of three SU(2) elements of size
+ * `su3eps` (or X^+ U, with probability 1/2, so the proposal is symmetric),
+ * accepted when exp(-dS) > r with dS = -(beta/3) Re tr[(U' - U) A].
+ * Starts from a cold, hot (Haar) or the current field.  Seeded and
+ * reproducible (counter-based Philox per link, sweep and hit); sweeps are
+ * numbered from the last cold/hot start, so a CURRENT call continues the
+ * chain (two calls of n sweeps equal one of 2n with the same seed).  Replaces the
+ * reference's GaugeFieldFactory update (src/Apps/gaugefieldfactory.cpp:192-220,
+ * src/Math/random.cpp:71-156), whose source does not compile.  FP32 forms are
+ * reunitarised in FP64 after every sweep.  *acceptance (optional) receives the
+ * accepted fraction.  Every extent must be even (YMFLOW_ERR_ARG otherwise). */
+YMFLOW_API int ymflow_generate_metropolis(ymflow_ctx* ctx, int start, double beta, double su3eps, int sweeps,
+                                          int hits, uint64_t seed, double* acceptance);
 
 /* Plaquette, clover energy and clover charge of the current links.
  * Replaces SuperObs::compute (src/Observables/superobs.cpp:31-128) including

@@ -26,13 +26,14 @@ NOALLOC_MAX_SITES = 8388608  # YMFLOW_NOALLOC_MAX_SITES
 
 FP64, FP32_18, FP32_12 = 0, 1, 2
 PRECISIONS = {"fp64": FP64, "fp32_18": FP32_18, "fp32_12": FP32_12}
-FIELD_COLD, FIELD_EXPIAH = 0, 1
+FIELD_COLD, FIELD_EXPIAH, FIELD_HOT, FIELD_CURRENT = 0, 1, 2, 3
 OPT_BLOCK, OPT_GRAPH, OPT_OBS_BLOCK = 1, 2, 3
 
 # every symbol include/ymflow.h declares
 EXPORTS = (
     "ymflow_version", "ymflow_device_count", "ymflow_create", "ymflow_destroy", "ymflow_last_error",
-    "ymflow_upload", "ymflow_download", "ymflow_init_links", "ymflow_observables", "ymflow_flow",
+    "ymflow_upload", "ymflow_download", "ymflow_init_links", "ymflow_generate_metropolis", "ymflow_observables",
+    "ymflow_flow",
     "ymflow_derivative", "ymflow_su3_exp", "ymflow_reset_time", "ymflow_time_steps", "ymflow_set_option", "ymflow_get_option",
     "ymflow_host_alloc", "ymflow_host_free", "ymflow_device_bytes",
     "ymflow_ensemble_create", "ymflow_ensemble_destroy", "ymflow_ensemble_last_error",
@@ -90,6 +91,8 @@ def load():
     l.ymflow_init_links.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint32,
                                     ctypes.c_double]
     l.ymflow_observables.argtypes = [vp, ctypes.POINTER(Obs)]
+    l.ymflow_generate_metropolis.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
     l.ymflow_flow.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                               ctypes.POINTER(Obs), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     l.ymflow_derivative.argtypes = [vp, ctypes.c_int, vp]

@@ -46,6 +46,12 @@ cudaError_t launch_init_links(int prec, void* u, const Geo& g, int kind, double 
 cudaError_t launch_haar_mix(int prec, void* u, const Geo& g, double frac, uint64_t seed, uint32_t config,
                             cudaStream_t st);
 
+// One checkerboard sub-sweep of Metropolis updates (generate.cu): every link
+// U_mu(x) with site parity `parity`, `hits` proposals each; accepted counts add
+// into *accepted.
+cudaError_t launch_metropolis(int prec, void* u, const Geo& g, int mu, int parity, double beta, double eps, int hits,
+                              uint64_t seed, uint32_t sweep, unsigned long long* accepted, cudaStream_t st);
+
 // FP64 Gram-Schmidt reunitarisation of every link; deviation[0] receives the
 // largest |row norm - 1| seen before the fix (as an ordered-int atomic max).
 cudaError_t launch_reunitarize(int prec, void* u, const Geo& g, unsigned long long* deviation, cudaStream_t st);

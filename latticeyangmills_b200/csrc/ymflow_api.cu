@@ -44,6 +44,7 @@ struct ymflow_ctx {
     bool loaded = false;
     int64_t step = 0;
     double t = 0.0;
+    uint32_t gen_sweep = 0;           // Metropolis sweeps since the last cold/hot start
     int64_t bytes = 0;
     std::string err;
 };
@@ -332,6 +333,47 @@ int ymflow_init_links(ymflow_ctx* c, int kind, double a, uint64_t seed, uint32_t
     if (haar_frac > 0.0)
         YM_CK(c, launch_haar_mix(c->prec, c->u[c->cur], c->geo, haar_frac, seed, config, c->stream), "haar launch");
     YM_CK(c, cudaStreamSynchronize(c->stream), "init links");
+    c->loaded = true;
+    c->step = 0;
+    c->t = 0.0;
+    return YMFLOW_OK;
+}
+
+int ymflow_generate_metropolis(ymflow_ctx* c, int start, double beta, double su3eps, int sweeps, int hits,
+                               uint64_t seed, double* acceptance) {
+    if (!c) return YMFLOW_ERR_ARG;
+    if (sweeps < 0 || hits < 1 || !(su3eps > 0.0 && su3eps < 1.0) || !std::isfinite(beta))
+        return fail(c, YMFLOW_ERR_ARG, "need sweeps >= 0, hits >= 1, 0 < su3eps < 1, finite beta");
+    if (start != YMFLOW_FIELD_COLD && start != YMFLOW_FIELD_HOT && start != YMFLOW_FIELD_CURRENT)
+        return fail(c, YMFLOW_ERR_ARG, "start must be COLD, HOT or CURRENT");
+    for (int i = 0; i < 4; i++)  // with an odd extent the periodic wrap joins two sites of one parity
+        if (c->dims[i] % 2) return fail(c, YMFLOW_ERR_ARG, "the checkerboard update needs even extents");
+    if (start == YMFLOW_FIELD_CURRENT && !c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    DeviceGuard guard(c->device);
+    if (start != YMFLOW_FIELD_CURRENT) {
+        YM_CK(c, launch_init_links(c->prec, c->u[c->cur], c->geo, kCold, 0.0, seed, 0, c->stream), "cold start");
+        if (start == YMFLOW_FIELD_HOT)
+            YM_CK(c, launch_haar_mix(c->prec, c->u[c->cur], c->geo, 1.0, seed, 0, c->stream), "hot start");
+        c->gen_sweep = 0;
+    }
+    YM_CK(c, cudaMemsetAsync(c->deviation, 0, sizeof(unsigned long long), c->stream), "reset counter");
+    for (int sw = 0; sw < sweeps; sw++) {
+        for (int mu = 0; mu < 4; mu++)
+            for (int parity = 0; parity < 2; parity++)
+                YM_CK(c, launch_metropolis(c->prec, c->u[c->cur], c->geo, mu, parity, beta, su3eps, hits, seed,
+                                           c->gen_sweep + uint32_t(sw), c->deviation, c->stream),
+                      "metropolis sweep");
+        if (c->prec != YMFLOW_FP64)
+            YM_CK(c, launch_reunitarize(c->prec, c->u[c->cur], c->geo, nullptr, c->stream), "reunitarise");
+    }
+    c->gen_sweep += uint32_t(sweeps);
+    unsigned long long acc = 0;
+    YM_CK(c, cudaMemcpyAsync(&acc, c->deviation, sizeof(acc), cudaMemcpyDeviceToHost, c->stream), "counter copy");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "generate");
+    if (acceptance) {
+        const double tries = double(sweeps) * double(hits) * 4.0 * double(c->geo.V);
+        *acceptance = tries > 0 ? double(acc) / tries : 0.0;
+    }
     c->loaded = true;
     c->step = 0;
     c->t = 0.0;

@@ -128,6 +128,17 @@ class GluonField:
         k = {"cold": N.FIELD_COLD, "expiah": N.FIELD_EXPIAH}[kind]
         self._check(N.load().ymflow_init_links(self.ctx, k, float(a), int(seed), int(config), float(haar_frac)))
 
+    def generate_metropolis(self, beta: float, su3eps: float = 0.24, sweeps: int = 200, hits: int = 30,
+                            seed: int = 1, start: str = "cold") -> float:
+        """Metropolis generation of the Wilson action (the reference's
+        GaugeFieldFactory update, src/Apps/gaugefieldfactory.cpp:192-220);
+        returns the acceptance."""
+        k = {"cold": N.FIELD_COLD, "hot": N.FIELD_HOT, "current": N.FIELD_CURRENT}[start]
+        acc = ctypes.c_double(0)
+        self._check(N.load().ymflow_generate_metropolis(self.ctx, k, float(beta), float(su3eps), int(sweeps),
+                                                        int(hits), int(seed), ctypes.byref(acc)))
+        return acc.value
+
     # compute
     def observables(self) -> N.Obs:
         o = N.Obs()

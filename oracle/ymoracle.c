@@ -618,6 +618,95 @@ double yo_gen_metropolis(double* U, const int n[4], double beta, double su3eps, 
     return tries ? (double)acc / (double)tries : 0.0;
 }
 
+/* The device generator's chain (test infrastructure for the checkerboard
+ * Metropolis kernel): the same update as yo_gen_metropolis, visited as a
+ * checkerboard -- sweep, then mu, then site parity, every link of that parity
+ * (their staples hold no link of the same direction and parity, so the order
+ * inside a parity class is immaterial) -- with the random numbers of
+ * (link l = 4 s + mu, sweep, hit) drawn counter-based: Philox4x32-10 with key
+ * (seed_lo, seed_hi ^ 0x4D455452) and counter (l_lo, l_hi ^ call << 24,
+ * sweep, hit) for call = 0..3; uniforms (w + 1/2) 2^-32; words 0-11 build the
+ * three SU(2) factors X = R S T, word 13 < 1/2 proposes X^+ U instead of X U
+ * (X and X^+ equally likely, so the proposal is symmetric and the chain keeps
+ * detailed balance, which R S T alone -- distributed unlike its inverse
+ * T^+ S^+ R^+ -- does not), word 12 is the accept draw.  dS is formed as
+ * -(beta/3) (Re tr U'A - Re tr UA).  Sweeps are numbered from sweep0. */
+static inline double unit32(uint32_t w) { return ((double)w + 0.5) * 2.3283064365386963e-10; }
+
+static void su2_from(const double r[4], double eps, int p, int q, double* m) {
+    double v1 = r[1] - 0.5, v2 = r[2] - 0.5, v3 = r[3] - 0.5;
+    const double norm = sqrt(v1 * v1 + v2 * v2 + v3 * v3);
+    const double x0 = (r[0] - 0.5 < 0.0 ? -1.0 : 1.0) * sqrt(1.0 - eps * eps);
+    v1 = v1 * eps / norm;
+    v2 = v2 * eps / norm;
+    v3 = v3 * eps / norm;
+    memset(m, 0, 18 * sizeof(double));
+    m[0] = m[8] = m[16] = 1.0;
+    m[2 * (3 * p + p)] = x0; m[2 * (3 * p + p) + 1] = v3;
+    m[2 * (3 * q + q)] = x0; m[2 * (3 * q + q) + 1] = -v3;
+    m[2 * (3 * p + q)] = v2; m[2 * (3 * p + q) + 1] = v1;
+    m[2 * (3 * q + p)] = -v2; m[2 * (3 * q + p) + 1] = v1;
+}
+
+static double re_trace_prod(const double* a, const double* b) {
+    double t = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) {
+            const double* x = a + 2 * (3 * i + k);
+            const double* y = b + 2 * (3 * k + i);
+            t += x[0] * y[0] - x[1] * y[1];
+        }
+    return t;
+}
+
+long yo_gen_metropolis_cb(double* U, const int n[4], double beta, double su3eps, int sweeps, int hits,
+                          uint64_t seed, uint32_t sweep0) {
+    const long V = volume(n);
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32) ^ 0x4D455452u};
+    long acc = 0;
+    for (int sw = 0; sw < sweeps; sw++)
+        for (int mu = 0; mu < 4; mu++)
+            for (int parity = 0; parity < 2; parity++)
+                for (long s = 0; s < V; s++) {
+                    int c[4];
+                    coords_of(n, s, c);
+                    if (((c[0] + c[1] + c[2] + c[3]) & 1) != parity) continue;
+                    double A[18];
+                    staple_site(U, n, s, mu, A);
+                    double* u = U + (s * 4 + mu) * 18;
+                    const uint64_t l = (uint64_t)s * 4 + (uint64_t)mu;
+                    for (int h = 0; h < hits; h++) {
+                        double r[16];
+                        for (uint32_t call = 0; call < 4; call++) {
+                            const uint32_t ctr[4] = {(uint32_t)l, (uint32_t)(l >> 32) ^ (call << 24),
+                                                     sweep0 + (uint32_t)sw, (uint32_t)h};
+                            uint32_t o[4];
+                            yo_philox4x32(ctr, key, o);
+                            for (int k = 0; k < 4; k++) r[4 * call + k] = unit32(o[k]);
+                        }
+                        double a[18], b[18], ab[18], X[18], un[18];
+                        su2_from(r + 0, su3eps, 0, 1, a);
+                        su2_from(r + 4, su3eps, 0, 2, b);
+                        yo_mul(a, b, ab);
+                        su2_from(r + 8, su3eps, 1, 2, a);
+                        yo_mul(ab, a, X);
+                        if (r[13] < 0.5) {
+                            double Xd[18];
+                            yo_dag(X, Xd);
+                            yo_mul(Xd, u, un);
+                        } else {
+                            yo_mul(X, u, un);
+                        }
+                        const double dS = -beta / 3.0 * (re_trace_prod(un, A) - re_trace_prod(u, A));
+                        if (exp(-dS) > r[12]) {
+                            memcpy(u, un, sizeof(un));
+                            acc++;
+                        }
+                    }
+                }
+    return acc;
+}
+
 /* Rows 0 and 1 normalised by Gram-Schmidt; row 2 = conj(row0 x row1). */
 void yo_reunitarize(double* U, long nlinks) {
 #pragma omp parallel for schedule(static)

@@ -46,6 +46,10 @@ void yo_gen_cold(double* U, const int n[4]);
  * own generator does not compile); returns the acceptance ratio. */
 double yo_gen_metropolis(double* U, const int n[4], double beta, double su3eps, int sweeps,
                          int hits, uint64_t seed);
+/* The device generator's checkerboard chain with counter-based random numbers
+ * (sweeps numbered from sweep0); returns the number of accepted proposals. */
+long yo_gen_metropolis_cb(double* U, const int n[4], double beta, double su3eps, int sweeps, int hits,
+                          uint64_t seed, uint32_t sweep0);
 /* FP64 Gram-Schmidt reunitarisation of nlinks 18-double links in place. */
 void yo_reunitarize(double* U, long nlinks);
 /* max over links of |U U^+ - 1| and |det U - 1|. */

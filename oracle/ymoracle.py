@@ -58,6 +58,9 @@ def lib():
         l.yo_gen_metropolis.argtypes = [_D, _I4, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_uint64]
         l.yo_gen_metropolis.restype = ctypes.c_double
+        l.yo_gen_metropolis_cb.argtypes = [_D, _I4, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32]
+        l.yo_gen_metropolis_cb.restype = ctypes.c_long
         l.yo_reunitarize.argtypes = [_D, ctypes.c_long]
         l.yo_unitarity.argtypes = [_D, ctypes.c_long, _D]
         _lib = l
@@ -102,6 +105,13 @@ def gen_metropolis(n, beta: float, su3eps: float, sweeps: int, hits: int, seed: 
     U = gen_cold(n)
     acc = lib().yo_gen_metropolis(_p(U), _dims(n), beta, su3eps, sweeps, hits, seed)
     return U, acc
+
+
+def gen_metropolis_cb(U: np.ndarray, n, beta: float, su3eps: float, sweeps: int, hits: int, seed: int,
+                      sweep0: int = 0) -> int:
+    """The device generator's checkerboard chain, in place on U; returns the
+    number of accepted proposals."""
+    return int(lib().yo_gen_metropolis_cb(_p(U), _dims(n), beta, su3eps, sweeps, hits, seed, sweep0))
 
 
 def su3_exp(q: np.ndarray) -> np.ndarray:

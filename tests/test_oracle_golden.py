@@ -116,3 +116,25 @@ def test_goldens_record_reference_schedule():
             if s % case["every"] == 0 or s == case["nsteps"]:
                 ts.append(t)
         np.testing.assert_array_equal(rows[:, 1], np.array(ts))
+
+
+def test_checkerboard_chain_properties(oracle):
+    """The device generator's chain on the CPU: beta = 0 accepts everything,
+    numbered sweeps continue a chain, and beta = 6 moves a cold field towards
+    the equilibrium plaquette while the links stay unitary."""
+    n = (4, 4, 4, 4)
+    V = oracle.volume(n)
+    U = oracle.gen_cold(n)
+    assert oracle.gen_metropolis_cb(U, n, 0.0, 0.24, 1, 3, 5) == 3 * 4 * V
+    a = oracle.gen_cold(n)
+    oracle.gen_metropolis_cb(a, n, 6.0, 0.24, 3, 4, 9)
+    b = oracle.gen_cold(n)
+    oracle.gen_metropolis_cb(b, n, 6.0, 0.24, 1, 4, 9)
+    oracle.gen_metropolis_cb(b, n, 6.0, 0.24, 2, 4, 9, sweep0=1)
+    assert np.array_equal(a, b)
+    c = oracle.gen_cold(n)
+    acc = oracle.gen_metropolis_cb(c, n, 6.0, 0.24, 40, 10, 3)
+    plaq = oracle.superobs(c, n)[0]
+    assert 0.08 < acc / (40 * 10 * 4 * V) < 0.2
+    assert 0.55 < plaq < 0.7
+    assert max(oracle.unitarity(c)) < 1e-12
