@@ -49,6 +49,13 @@ def bytes_per_link_update(prec: str) -> int:
     return 6 * LINK_BYTES[prec] + 4 * FORCE_BYTES[prec]
 
 
+# Algorithmic flops of one link through one RK3 stage, as the reference's
+# algorithm counts them: 12 staple products + U Omega + Q^2 + e^{iQ} U, 198 flops
+# per 3x3 complex product, plus about 300 scalar flops (projection, RK combine,
+# tr Q^3, Cayley-Hamilton coefficients, f0 + f1 Q + f2 Q^2).
+FLOPS_PER_LINK_STAGE = 15 * 198 + 300
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -386,6 +393,10 @@ def our_arm(args, dist: Dist):
     avg_launch_s = kernel_ms / 1e3 / (3 * args.steps)
     achieved = bpl / avg_launch_s / 1e9
     traffic = profiled_traffic(prec, DIMS, bpl)
+    # arithmetic roofline: the same launches against the measured CUDA-core FMA peak
+    fma_tf = ctypes.c_double(0.0)
+    N.check(N.load().ymflow_fma_peak(dev, N.FP64 if prec == "fp64" else N.FP32_18, ctypes.byref(fma_tf)))
+    alu_achieved = links * FLOPS_PER_LINK_STAGE / avg_launch_s / 1e12
 
     # accuracy of the mixed form against FP64 at t = 4 (400 steps), same seeded field
     accuracy = None
@@ -455,6 +466,10 @@ def our_arm(args, dist: Dist):
                          "kernel": "rk_stage_kernel (fused RK3 stage)",
                          "algorithmic_bytes_per_launch": bpl,
                          "avg_launch_ms": avg_launch_s * 1e3},
+            "alu_roofline": {"bound": "fp64 fma" if prec == "fp64" else "fp32 fma", "achieved": alu_achieved,
+                             "peak": fma_tf.value, "unit": "TFLOP/s", "frac": alu_achieved / fma_tf.value,
+                             "peak_kind": "measured (ymflow_fma_peak, 8 independent FMA chains per thread)",
+                             "flops_per_link_update": 3 * FLOPS_PER_LINK_STAGE},
             "accuracy_vs_fp64": accuracy,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes / args.steps,
                     "d2h_bytes_per_step": rows_bytes / args.steps,

@@ -99,6 +99,22 @@ YMFLOW_API int ymflow_upload(ymflow_ctx* ctx, const double* links_aos);
  * (The reference's writer is a no-op, src/InputOutput/outputconf.cpp:102.) */
 YMFLOW_API int ymflow_download(ymflow_ctx* ctx, double* links_aos);
 
+/* Ranged transfers for large lattices: sites [first_site, first_site + nsites)
+ * in the .bin layout (links_aos points at site first_site's first double), so a
+ * caller can stream a configuration file through a small (ideally pinned,
+ * ymflow_host_alloc) buffer instead of holding the whole field in host memory.
+ * flags: YMFLOW_IO_BIG_ENDIAN = every double byte-reversed, the big-endian
+ * ("Chroma") files of the reference's commented reader variant
+ * (src/InputOutput/inputconf.cpp:135-143); the reversal runs on the device.
+ * An upload marks the field loaded and resets the flow time; the caller covers
+ * every site before flowing.  Synchronous like ymflow_upload/ymflow_download;
+ * the device staging buffer grows to the largest range used. */
+#define YMFLOW_IO_BIG_ENDIAN 1
+YMFLOW_API int ymflow_upload_sites(ymflow_ctx* ctx, const double* links_aos, int64_t first_site, int64_t nsites,
+                                   int flags);
+YMFLOW_API int ymflow_download_sites(ymflow_ctx* ctx, double* links_aos, int64_t first_site, int64_t nsites,
+                                     int flags);
+
 /* Fill the links with a seeded synthetic field on the device: kind COLD or
  * EXPIAH (scale a); then, if haar_frac > 0, replace that fraction of links
  * (seeded Bernoulli) by Haar-random SU(3).  Same recipe as the test fixtures. */
@@ -170,6 +186,12 @@ YMFLOW_API int ymflow_time_steps(ymflow_ctx* ctx, double eps, int nsteps, float*
 #define YMFLOW_OPT_OBS_BLOCK 3
 YMFLOW_API int ymflow_set_option(ymflow_ctx* ctx, int key, int64_t value);
 YMFLOW_API int ymflow_get_option(const ymflow_ctx* ctx, int key, int64_t* value);
+
+/* Measured CUDA-core FMA throughput of `device` in TFLOP/s (2 flops per FMA):
+ * FP64 FMAs for YMFLOW_FP64, FP32 FMAs otherwise.  A measurement utility with
+ * no counterpart in the reference: the denominator of the stage kernels'
+ * arithmetic roofline.  Runs twelve short kernels (about 0.1 s); best of eleven. */
+YMFLOW_API int ymflow_fma_peak(int device, int precision, double* tflops);
 
 /* Page-locked host memory for transfers at full PCIe rate (cudaMallocHost). */
 YMFLOW_API int ymflow_host_alloc(int64_t bytes, void** ptr);

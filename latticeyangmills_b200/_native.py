@@ -27,15 +27,16 @@ NOALLOC_MAX_SITES = 8388608  # YMFLOW_NOALLOC_MAX_SITES
 FP64, FP32_18, FP32_12 = 0, 1, 2
 PRECISIONS = {"fp64": FP64, "fp32_18": FP32_18, "fp32_12": FP32_12}
 FIELD_COLD, FIELD_EXPIAH, FIELD_HOT, FIELD_CURRENT = 0, 1, 2, 3
+IO_BIG_ENDIAN = 1
 OPT_BLOCK, OPT_GRAPH, OPT_OBS_BLOCK = 1, 2, 3
 
 # every symbol include/ymflow.h declares
 EXPORTS = (
     "ymflow_version", "ymflow_device_count", "ymflow_create", "ymflow_destroy", "ymflow_last_error",
-    "ymflow_upload", "ymflow_download", "ymflow_init_links", "ymflow_generate_metropolis", "ymflow_observables",
-    "ymflow_flow",
-    "ymflow_derivative", "ymflow_su3_exp", "ymflow_reset_time", "ymflow_time_steps", "ymflow_set_option", "ymflow_get_option",
-    "ymflow_host_alloc", "ymflow_host_free", "ymflow_device_bytes",
+    "ymflow_upload", "ymflow_download", "ymflow_upload_sites", "ymflow_download_sites", "ymflow_init_links",
+    "ymflow_generate_metropolis", "ymflow_observables", "ymflow_flow", "ymflow_derivative", "ymflow_su3_exp",
+    "ymflow_reset_time", "ymflow_time_steps", "ymflow_set_option", "ymflow_get_option",
+    "ymflow_host_alloc", "ymflow_host_free", "ymflow_device_bytes", "ymflow_fma_peak",
     "ymflow_ensemble_create", "ymflow_ensemble_destroy", "ymflow_ensemble_last_error",
     "ymflow_ensemble_upload", "ymflow_ensemble_download", "ymflow_ensemble_init_links",
     "ymflow_ensemble_flow", "ymflow_ensemble_reset_time", "ymflow_ensemble_time_steps",
@@ -91,6 +92,9 @@ def load():
     l.ymflow_init_links.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint32,
                                     ctypes.c_double]
     l.ymflow_observables.argtypes = [vp, ctypes.POINTER(Obs)]
+    l.ymflow_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    l.ymflow_upload_sites.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
+    l.ymflow_download_sites.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
     l.ymflow_generate_metropolis.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
     l.ymflow_flow.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -11,7 +11,14 @@
 //   "InputDir", "OutputDir"                                             (jsondirectories.cpp:20-55)
 // Optional keys this driver adds, outside App.params (whose size the reference
 // checks): "Precision" ("fp64" default, "fp32_18", "fp32_12"), "ReunitEvery"
-// (mixed precisions, default 10), "Device" (default 0).
+// (mixed precisions, default 10), "Device" (default 0), "Endian" ("little"
+// default; "big" reads the byte-reversed files of the reference's commented
+// "FOR CHROMA" reader, inputconf.cpp:135-143), "IOChunkSites" (sites per
+// streamed read, default 65536).
+//
+// Configurations are streamed: each file is read in chunks into one pinned
+// buffer and uploaded range by range (byte reversal on the device), so no
+// whole-field host copy is held (a 64^4 .bin is 9.7 GB).
 //
 // Same inputs and outputs: every *.bin in InputDir in sorted order
 // (inputconf.cpp:76-82), int(tauFinal/epsilon) rows per configuration with
@@ -56,6 +63,8 @@ struct Input {
     int precision = YMFLOW_FP64;
     int reunit_every = 10;
     int device = 0;
+    bool big_endian = false;
+    int64_t chunk_sites = 65536;
 };
 
 void read_extents(const jl::Value& root, const char* key, int out[4]) {
@@ -134,6 +143,15 @@ Input parse_input(const char* path) {
     }
     if (root.count("ReunitEvery")) in.reunit_every = int(root["ReunitEvery"].num);
     if (root.count("Device")) in.device = int(root["Device"].num);
+    if (root.count("Endian")) {
+        const std::string e = root["Endian"].str;
+        if (e == "big") in.big_endian = true;
+        else if (e != "little") die("unknown Endian \"" + e + "\" (little, big)");
+    }
+    if (root.count("IOChunkSites")) {
+        in.chunk_sites = int64_t(root["IOChunkSites"].num);
+        if (in.chunk_sites < 1) die("IOChunkSites must be >= 1");
+    }
     if (!(in.epsilon > 0.0) || !(in.tau_final >= 0.0)) die("epsilon must be > 0 and tauFinal >= 0");
     return in;
 }
@@ -181,7 +199,11 @@ int main(int argc, char** argv) {
     if (!ctx) die(std::string("ymflow_create: ") + ymflow_last_error(nullptr));
 
     const int64_t V = int64_t(in.size[0]) * in.size[1] * in.size[2] * in.size[3];
-    std::vector<double> links(size_t(V) * 4 * 18);
+    const int64_t chunk = std::min<int64_t>(in.chunk_sites, V);
+    void* pinned = nullptr;
+    if (ymflow_host_alloc(chunk * 72 * int64_t(sizeof(double)), &pinned) != YMFLOW_OK || !pinned)
+        die("cannot allocate the pinned read buffer");
+    double* buf = static_cast<double*>(pinned);
     const int rows = int(in.tau_final / in.epsilon);  // wilsonflow.cpp:117
     const int nsteps = rows > 1 ? rows - 1 : 0;
     std::vector<ymflow_obs> obs(size_t(nsteps) + 2);
@@ -190,10 +212,16 @@ int main(int argc, char** argv) {
     for (const std::string& path : input_list(in.input_dir)) {
         FILE* f = std::fopen(path.c_str(), "rb");
         if (!f) die("cannot open " + path);
-        const size_t got = std::fread(links.data(), sizeof(double), links.size(), f);
+        for (int64_t first = 0; first < V; first += chunk) {
+            const int64_t n = std::min(chunk, V - first);
+            const size_t want = size_t(n) * 72;
+            if (std::fread(buf, sizeof(double), want, f) != want) {
+                std::fclose(f);
+                die(path + ": shorter than the LatticeSize configuration");
+            }
+            check(ymflow_upload_sites(ctx, buf, first, n, in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0), ctx, "upload");
+        }
         std::fclose(f);
-        if (got != links.size()) die(path + ": shorter than the LatticeSize configuration");
-        check(ymflow_upload(ctx, links.data()), ctx, "upload");
         int n_out = 0;
         check(ymflow_flow(ctx, in.epsilon, nsteps, 1, in.reunit_every, obs.data(), int(obs.size()), &n_out), ctx,
               "flow");
@@ -233,6 +261,7 @@ int main(int argc, char** argv) {
         }
         conf_num++;
     }
+    ymflow_host_free(buf);
     ymflow_destroy(ctx);
     const std::chrono::duration<double> el = std::chrono::system_clock::now() - start;
     std::printf("Total time taken: %.2fs\n", el.count());

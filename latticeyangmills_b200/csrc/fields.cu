@@ -9,56 +9,87 @@ namespace ym {
 // src/InputOutput/inputconf.cpp:114-155) <-> the device SoA layout.
 // One thread per link; the AoS side is read/written 16 bytes at a time.
 // ---------------------------------------------------------------------------
+// A .bin double with its bytes reversed (the big-endian "Chroma" files that
+// inputconf.cpp:135-143 reads with ReverseDouble).
+__device__ __forceinline__ double reverse_bytes(double x) {
+    const unsigned long long v = (unsigned long long)__double_as_longlong(x);
+    const uint32_t lo = __byte_perm(uint32_t(v >> 32), 0u, 0x0123);
+    const uint32_t hi = __byte_perm(uint32_t(v), 0u, 0x0123);
+    return __longlong_as_double((long long)((uint64_t(hi) << 32) | lo));
+}
+
+// Sites [first, first + n) of a .bin-layout block (aos points at site `first`).
 template <class F>
-__global__ void pack_kernel(const double* __restrict__ aos, F u, int V) {
+__global__ void pack_kernel(const double* __restrict__ aos, F u, int first, int n, bool swap) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * int64_t(V)) return;
-    const int s = int(l >> 2);
+    if (l >= 4 * int64_t(n)) return;
+    const int s = first + int(l >> 2);
     const int mu = int(l & 3);
     const double2* src = reinterpret_cast<const double2*>(aos + l * 18);
     M3<typename F::Real> a;
 #pragma unroll
     for (int e = 0; e < 9; e++) {
-        const double2 v = src[e];
+        double2 v = src[e];
+        if (swap) v = make_double2(reverse_bytes(v.x), reverse_bytes(v.y));
         a.e[e / 3][e % 3] = cx(typename F::Real(v.x), typename F::Real(v.y));
     }
     u.store(mu, s, a);
 }
 
 template <class F>
-__global__ void unpack_kernel(F u, double* __restrict__ aos, int V) {
+__global__ void unpack_kernel(F u, double* __restrict__ aos, int first, int n, bool swap) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * int64_t(V)) return;
-    const int s = int(l >> 2);
+    if (l >= 4 * int64_t(n)) return;
+    const int s = first + int(l >> 2);
     const int mu = int(l & 3);
     const M3<typename F::Real> a = u.load(mu, s);
     double2* dst = reinterpret_cast<double2*>(aos + l * 18);
 #pragma unroll
-    for (int e = 0; e < 9; e++) dst[e] = make_double2(double(a.e[e / 3][e % 3].re), double(a.e[e / 3][e % 3].im));
+    for (int e = 0; e < 9; e++) {
+        double2 v = make_double2(double(a.e[e / 3][e % 3].re), double(a.e[e / 3][e % 3].im));
+        if (swap) v = make_double2(reverse_bytes(v.x), reverse_bytes(v.y));
+        dst[e] = v;
+    }
+}
+
+cudaError_t launch_pack_range(int prec, const double* aos, void* u, const Geo& g, int first, int n, bool swap,
+                              cudaStream_t st) {
+    if (first < 0 || n < 0 || int64_t(first) + n > g.V) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    const int b = 256;
+    const unsigned nb = unsigned((4 * int64_t(n) + b - 1) / b);
+    void* v = const_cast<void*>((const void*)u);
+    switch (prec) {
+        case kFP64: pack_kernel<<<nb, b, 0, st>>>(aos, FieldD18{v, g.V}, first, n, swap); break;
+        case kFP32_18: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF18{v, g.V}, first, n, swap); break;
+        case kFP32_12: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF12{v, g.V}, first, n, swap); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_range(int prec, const void* u, double* aos, const Geo& g, int first, int n, bool swap,
+                                cudaStream_t st) {
+    if (first < 0 || n < 0 || int64_t(first) + n > g.V) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    const int b = 256;
+    const unsigned nb = unsigned((4 * int64_t(n) + b - 1) / b);
+    void* v = const_cast<void*>(u);
+    switch (prec) {
+        case kFP64: unpack_kernel<<<nb, b, 0, st>>>(FieldD18{v, g.V}, aos, first, n, swap); break;
+        case kFP32_18: unpack_kernel<<<nb, b, 0, st>>>(FieldF18{v, g.V}, aos, first, n, swap); break;
+        case kFP32_12: unpack_kernel<<<nb, b, 0, st>>>(FieldF12{v, g.V}, aos, first, n, swap); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_pack(int prec, const double* aos, void* u, const Geo& g, cudaStream_t st) {
-    const int b = 256;
-    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
-    switch (prec) {
-        case kFP64: pack_kernel<<<nb, b, 0, st>>>(aos, FieldD18{const_cast<void*>((const void*)u), g.V}, g.V); break;
-        case kFP32_18: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF18{const_cast<void*>((const void*)u), g.V}, g.V); break;
-        case kFP32_12: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF12{const_cast<void*>((const void*)u), g.V}, g.V); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    return launch_pack_range(prec, aos, u, g, 0, g.V, false, st);
 }
 
 cudaError_t launch_unpack(int prec, const void* u, double* aos, const Geo& g, cudaStream_t st) {
-    const int b = 256;
-    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
-    switch (prec) {
-        case kFP64: unpack_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, aos, g.V); break;
-        case kFP32_18: unpack_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, aos, g.V); break;
-        case kFP32_12: unpack_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, aos, g.V); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    return launch_unpack_range(prec, u, aos, g, 0, g.V, false, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -36,6 +36,12 @@ cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* pa
 cudaError_t launch_obs_finalize(const double* partials, int nblocks, const Geo& g, double* out, cudaStream_t st);
 
 // .bin layout (site-major, mu, 18 doubles) <-> device layout
+// Sites [first, first + n) between a .bin-layout block (aos points at site
+// `first`) and the device links; swap = each double byte-reversed.
+cudaError_t launch_pack_range(int prec, const double* aos, void* u, const Geo& g, int first, int n, bool swap,
+                              cudaStream_t st);
+cudaError_t launch_unpack_range(int prec, const void* u, double* aos, const Geo& g, int first, int n, bool swap,
+                                cudaStream_t st);
 cudaError_t launch_pack(int prec, const double* aos, void* u, const Geo& g, cudaStream_t st);
 cudaError_t launch_unpack(int prec, const void* u, double* aos, const Geo& g, cudaStream_t st);
 

@@ -27,6 +27,7 @@ struct ymflow_ctx {
     int cur = 0;                      // which of u[] holds the current field
     void* z = nullptr;                // RK generator, 8 reals per link
     double* staging = nullptr;        // .bin-layout device buffer for upload/download
+    size_t staging_bytes = 0;
     double* partials = nullptr;       // observables: 3 doubles per block
     int partial_cap = 0;
     double* meas = nullptr;           // measurement rows on the device, 4 doubles each
@@ -79,9 +80,19 @@ int dev_alloc(ymflow_ctx* c, void** p, size_t bytes, const char* what) {
     return YMFLOW_OK;
 }
 
-int ensure_staging(ymflow_ctx* c) {
-    if (c->staging) return YMFLOW_OK;
-    return dev_alloc(c, (void**)&c->staging, size_t(link_count(c)) * 18 * sizeof(double), "staging buffer");
+// .bin-layout device buffer of at least `bytes` (the whole field by default)
+int ensure_staging(ymflow_ctx* c, size_t bytes = 0) {
+    if (bytes == 0) bytes = size_t(link_count(c)) * 18 * sizeof(double);
+    if (c->staging && c->staging_bytes >= bytes) return YMFLOW_OK;
+    if (c->staging) {
+        cudaFree(c->staging);
+        c->bytes -= int64_t(c->staging_bytes);
+        c->staging = nullptr;
+        c->staging_bytes = 0;
+    }
+    const int r = dev_alloc(c, (void**)&c->staging, bytes, "staging buffer");
+    if (r == YMFLOW_OK) c->staging_bytes = bytes;
+    return r;
 }
 
 int ensure_partials(ymflow_ctx* c) {
@@ -317,6 +328,54 @@ int ymflow_download(ymflow_ctx* c, double* links) {
     if (r != YMFLOW_OK) return r;
     const size_t bytes = size_t(link_count(c)) * 18 * sizeof(double);
     YM_CK(c, launch_unpack(c->prec, c->u[c->cur], c->staging, c->geo, c->stream), "unpack launch");
+    YM_CK(c, cudaMemcpyAsync(links, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream), "download copy");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "download");
+    return YMFLOW_OK;
+}
+
+namespace {
+
+int check_site_range(ymflow_ctx* c, const void* p, int64_t first, int64_t n, int flags) {
+    if (!c) return YMFLOW_ERR_ARG;
+    if (!p && n > 0) return fail(c, YMFLOW_ERR_ARG, "null links pointer");
+    if (first < 0 || n < 0 || first + n > int64_t(c->geo.V))
+        return fail(c, YMFLOW_ERR_ARG, "site range outside the lattice");
+    if (flags & ~YMFLOW_IO_BIG_ENDIAN) return fail(c, YMFLOW_ERR_ARG, "unknown flags");
+    return YMFLOW_OK;
+}
+
+}  // namespace
+
+int ymflow_upload_sites(ymflow_ctx* c, const double* links, int64_t first_site, int64_t nsites, int flags) {
+    int r = check_site_range(c, links, first_site, nsites, flags);
+    if (r != YMFLOW_OK || nsites == 0) return r;
+    DeviceGuard guard(c->device);
+    const size_t bytes = size_t(nsites) * 4 * 18 * sizeof(double);
+    r = ensure_staging(c, bytes);
+    if (r != YMFLOW_OK) return r;
+    YM_CK(c, cudaMemcpyAsync(c->staging, links, bytes, cudaMemcpyHostToDevice, c->stream), "upload copy");
+    YM_CK(c, launch_pack_range(c->prec, c->staging, c->u[c->cur], c->geo, int(first_site), int(nsites),
+                               (flags & YMFLOW_IO_BIG_ENDIAN) != 0, c->stream),
+          "pack launch");
+    YM_CK(c, cudaStreamSynchronize(c->stream), "upload");
+    c->loaded = true;
+    c->step = 0;
+    c->t = 0.0;
+    return YMFLOW_OK;
+}
+
+int ymflow_download_sites(ymflow_ctx* c, double* links, int64_t first_site, int64_t nsites, int flags) {
+    int r = check_site_range(c, links, first_site, nsites, flags);
+    if (r != YMFLOW_OK) return r;
+    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    if (nsites == 0) return YMFLOW_OK;
+    DeviceGuard guard(c->device);
+    const size_t bytes = size_t(nsites) * 4 * 18 * sizeof(double);
+    r = ensure_staging(c, bytes);
+    if (r != YMFLOW_OK) return r;
+    YM_CK(c, launch_unpack_range(c->prec, c->u[c->cur], c->staging, c->geo, int(first_site), int(nsites),
+                                 (flags & YMFLOW_IO_BIG_ENDIAN) != 0, c->stream),
+          "unpack launch");
     YM_CK(c, cudaMemcpyAsync(links, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream), "download copy");
     YM_CK(c, cudaStreamSynchronize(c->stream), "download");
     return YMFLOW_OK;

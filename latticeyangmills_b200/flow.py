@@ -34,21 +34,22 @@ def volume(size: Sequence[int]) -> int:
     return int(size[0]) * int(size[1]) * int(size[2]) * int(size[3])
 
 
-def read_conf(path, size: Sequence[int]) -> np.ndarray:
-    """Links of a .bin configuration: raw native-endian doubles, per global site
-    (x fastest) 4 links of 18 doubles (inputconf.cpp:114-155).  Shape
-    (Nt, Nz, Ny, Nx, 4, 18)."""
+def read_conf(path, size: Sequence[int], big_endian: bool = False) -> np.ndarray:
+    """Links of a .bin configuration: raw doubles, per global site (x fastest) 4
+    links of 18 doubles (inputconf.cpp:114-155); big_endian reads the
+    byte-reversed "Chroma" variant (inputconf.cpp:135-143).  Shape
+    (Nt, Nz, Ny, Nx, 4, 18), native byte order."""
     n = volume(size) * 4 * 18
-    a = np.fromfile(str(path), dtype=np.float64)
+    a = np.fromfile(str(path), dtype=">f8" if big_endian else "<f8")
     if a.size != n:
         raise ValueError(f"{path}: {a.size * 8} bytes, expected {n * 8} for lattice {tuple(size)}")
-    return a.reshape(size[3], size[2], size[1], size[0], 4, 18)
+    return a.astype(np.float64).reshape(size[3], size[2], size[1], size[0], 4, 18)
 
 
-def write_conf(path, links: np.ndarray) -> None:
+def write_conf(path, links: np.ndarray, big_endian: bool = False) -> None:
     """Writes links in the .bin layout read_conf reads (the reference's writer
     is a no-op, src/InputOutput/outputconf.cpp:102)."""
-    np.ascontiguousarray(links, dtype=np.float64).tofile(str(path))
+    np.ascontiguousarray(links, dtype=">f8" if big_endian else "<f8").tofile(str(path))
 
 
 def get_input_list(input_dir) -> List[str]:
@@ -122,6 +123,33 @@ class GluonField:
         a = np.empty((self.size[3], self.size[2], self.size[1], self.size[0], 4, 18), dtype=np.float64)
         self._check(N.load().ymflow_download(self.ctx, a.ctypes.data))
         return a
+
+    def upload_sites(self, links: np.ndarray, first_site: int) -> None:
+        """Sites [first_site, first_site + n) from a .bin-layout block of n*72
+        doubles, little- or big-endian (">f8": byte-reversed on the device)."""
+        a = np.ascontiguousarray(links)
+        if a.dtype not in (np.dtype("<f8"), np.dtype(">f8")) or a.size % 72:
+            raise ValueError("links must be float64 with 72 doubles per site")
+        flags = N.IO_BIG_ENDIAN if a.dtype.byteorder == ">" else 0
+        self._check(N.load().ymflow_upload_sites(self.ctx, a.ctypes.data, int(first_site), a.size // 72, flags))
+
+    def download_sites(self, first_site: int, nsites: int, big_endian: bool = False) -> np.ndarray:
+        a = np.empty((int(nsites), 4, 18), dtype=">f8" if big_endian else "<f8")
+        flags = N.IO_BIG_ENDIAN if big_endian else 0
+        self._check(N.load().ymflow_download_sites(self.ctx, a.ctypes.data, int(first_site), int(nsites), flags))
+        return a
+
+    def load_conf(self, path, big_endian: bool = False, chunk_sites: int = 65536) -> None:
+        """Streams a .bin file into the field chunk by chunk (no whole-field host copy)."""
+        V = self.sites
+        size = Path(path).stat().st_size
+        if size != V * 72 * 8:
+            raise ValueError(f"{path}: {size} bytes, expected {V * 72 * 8}")
+        dt = ">f8" if big_endian else "<f8"
+        with open(path, "rb") as fh:
+            for first in range(0, V, chunk_sites):
+                n = min(chunk_sites, V - first)
+                self.upload_sites(np.fromfile(fh, dtype=dt, count=n * 72), first)
 
     def init_links(self, kind: str = "expiah", a: float = 0.35, seed: int = 1, config: int = 0,
                    haar_frac: float = 0.0) -> None:

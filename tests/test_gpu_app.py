@@ -41,6 +41,23 @@ def test_flow_app_output_matches_reference_app(tmp_path):
     assert (tmp_path / "out" / "flow" / "conf0000.full.dat").exists()
 
 
+def test_flow_app_big_endian_streamed_input(tmp_path):
+    """Byte-reversed ("Chroma") inputs read in ragged chunks give the same
+    files as the native-endian run."""
+    import numpy as np
+
+    run = prepare(tmp_path, {"Endian": "big", "IOChunkSites": 97})
+    for name in ["conf0000.bin", "conf0001.bin"]:
+        f = tmp_path / "in" / name
+        f.write_bytes(np.fromfile(f, dtype="<f8").astype(">f8").tobytes())
+    res = subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)
+    got = [l for l in res.stdout.splitlines(keepends=True) if not l.startswith("Total time taken")]
+    exp = GOLDEN / "app_flow" / "expected"
+    assert "".join(got) == (exp / "stdout.txt").read_text()
+    for f in ["observables.dat", "flow/conf0000.dat", "flow/conf0001.dat"]:
+        assert (tmp_path / "out" / f).read_bytes() == (exp / f).read_bytes(), f
+
+
 def test_flow_app_mixed_precision_rows(tmp_path):
     run = prepare(tmp_path, {"Precision": "fp32_12", "ReunitEvery": 5})
     subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)

@@ -67,3 +67,19 @@ def test_wrong_size_upload_rejected_on_host():
     with GluonField((4, 4, 4, 4)) as f:
         with pytest.raises(ValueError):
             f.upload(np.zeros(10))
+
+
+def test_fma_peak_is_measured():
+    import ctypes
+
+    from latticeyangmills_b200 import _native as N
+
+    tf = {}
+    for p in (N.FP32_18, N.FP64):
+        v = ctypes.c_double(0.0)
+        assert N.load().ymflow_fma_peak(0, p, ctypes.byref(v)) == N.OK
+        tf[p] = v.value
+    print("FMA peak TFLOP/s: fp32", tf[N.FP32_18], "fp64", tf[N.FP64])
+    assert 20.0 < tf[N.FP32_18] < 200.0
+    assert 5.0 < tf[N.FP64] < tf[N.FP32_18]
+    assert N.load().ymflow_fma_peak(0, 7, ctypes.byref(ctypes.c_double())) == N.ERR_ARG

@@ -70,9 +70,23 @@ def _app_input(tmp_path, extra):
     ({"Observables": ["wilsonloop"]}, "unknown Observable"),
     ({"LatticeSize": {"x": 4, "y": 4, "z": 4}}, "wrong LatticeSize specification"),
     ({"Precision": "fp16"}, "unknown Precision"),
+    ({"Endian": "middle"}, "unknown Endian"),
+    ({"IOChunkSites": 0}, "IOChunkSites must be >= 1"),
 ])
 def test_flow_app_rejects_bad_input(tmp_path, bad, msg):
     # validation as the reference's JsonInput layer, before any device work
     run = _app_input(tmp_path, bad)
     res = subprocess.run([str(APP), str(run)], capture_output=True, text=True)
     assert res.returncode == 1 and msg in res.stderr
+
+
+def test_big_endian_conf_round_trip(tmp_path):
+    from latticeyangmills_b200 import read_conf, write_conf
+
+    n = (4, 4, 4, 4)
+    U = read_conf(GOLDEN / "g4_expiah.bin", n)
+    write_conf(tmp_path / "be.bin", U, big_endian=True)
+    raw = (tmp_path / "be.bin").read_bytes()
+    assert raw[:8] == U.reshape(-1)[:1].astype(">f8").tobytes()
+    assert raw != (GOLDEN / "g4_expiah.bin").read_bytes()
+    assert np.array_equal(read_conf(tmp_path / "be.bin", n, big_endian=True), U)
