@@ -344,8 +344,8 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
             }
             V *= d[i];
         }
-        if (V >= (int64_t(1) << 31)) {
-            set(YMFLOW_ERR_ARG, "configuration " + std::to_string(c) + ": volume must be below 2^31 sites");
+        if (V >= (int64_t(1) << 31) || !volume_addressable(precision, V)) {
+            set(YMFLOW_ERR_ARG, "configuration " + std::to_string(c) + ": volume too large");
             delete e;
             return nullptr;
         }
@@ -353,8 +353,8 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
         C.g = make_geo(d);
         C.uoff = uo;
         C.zoff = zo;
-        uo += int64_t(4) * int64_t(link_bytes(e->prec)) * V;
-        zo += int64_t(4) * int64_t(force_bytes(e->prec)) * V;
+        uo += int64_t(link_field_bytes(e->prec, V));
+        zo += int64_t(force_field_bytes(e->prec, V));
         e->max_v = std::max(e->max_v, V);
         e->signature += std::to_string(d[0]) + "x" + std::to_string(d[1]) + "x" + std::to_string(d[2]) + "x" +
                         std::to_string(d[3]) + ";";

@@ -1,15 +1,22 @@
 // Device storage of gauge fields and flow generators, and the lattice geometry.
 //
-// HBM layout: structure of arrays, so that a warp's 32 consecutive sites read
-// 32 consecutive 16-byte vectors per load instruction.
+// HBM layout: sites in groups of 32 (one warp's sites), structure of arrays
+// inside a group.  For each (mu, group) the link components are consecutive
+// 512-byte blocks, each holding one 16-byte vector for the 32 sites:
 //
-//   FP64 links   double2 plane per (mu, element e): 9 planes of V entries per mu
-//   FP32 links   float4 plane per (mu, element pair): elements (0,1) (2,3) (4,5)
-//                for the two-row 12-real form (3 planes per mu); the 18-real form
-//                adds (6,7) and a float2 plane for element 8 (placed after all
-//                float4 planes so every plane stays 16-byte aligned)
+//   FP64 links   9 double2 blocks: element e of the 32 sites
+//   FP32 links   float4 blocks of element pairs (0,1) (2,3) (4,5) for the
+//                two-row 12-real form; the 18-real form adds (6,7) and a
+//                256-byte float2 block for element 8
 //   generator    the Hermitian traceless Z as 8 reals (Herm8: Z00, Z11, Re/Im Z01,
-//                Z02, Z12): 4 double2 or 2 float4 planes per mu
+//                Z02, Z12): 4 double2 or 2 float4 blocks
+//
+// A warp's 32 consecutive sites read 512 contiguous bytes per load
+// instruction, and the blocks of one link are at fixed offsets from one
+// address, so a link costs one address computation whatever its number of
+// vectors.  Groups run over [mu][group]; the volume is padded to a multiple of
+// 32 sites (padding lanes are never read).  Offsets are 32-bit counts of
+// 16-byte units (the context checks 4 x padded V x link bytes / 16 < 2^32).
 //
 // Elements are row-major, (re, im); the two-row form stores rows 0 and 1 and
 // rebuilds row 2 = conj(row0 x row1) on load.  Site order is the reference's
@@ -98,6 +105,15 @@ inline Geo make_geo(const int dims[4]) {
     return g;
 }
 
+inline int64_t padded_sites(int64_t V) { return (V + 31) & ~int64_t(31); }
+
+// First 16-byte unit of the (mu, group of s) block run, plus the lane of s;
+// `units` = 16-byte units per group (32 x bytes per link / 16).
+__device__ __forceinline__ uint32_t group_lane_unit(int mu, int s, int V, int units) {
+    const int groups = (V + 31) >> 5;
+    return uint32_t(mu * groups + (s >> 5)) * uint32_t(units) + uint32_t(s & 31);
+}
+
 template <class R>
 __device__ __forceinline__ void set_elem(M3<R>& a, int e, R re, R im) {
     a.e[e / 3][e % 3] = cx(re, im);
@@ -111,45 +127,54 @@ template <int NE>
 struct LinkField<double, NE> {
     using Real = double;
     static constexpr int kElems = NE;
+    static constexpr int kUnits = NE * 32;  // 16-byte units per group
     void* p;
     int V;
 
-    __device__ __forceinline__ const double2* plane(int mu, int e) const {
-        return reinterpret_cast<const double2*>(p) + int64_t(mu * NE + e) * V;
+    // element 0 of link (mu, s); element e is 32 units further per e
+    __device__ __forceinline__ const double2* link(int mu, int s) const {
+        return reinterpret_cast<const double2*>(p) + group_lane_unit(mu, s, V, kUnits);
     }
     __device__ __forceinline__ Rows2<double> load_rows2(int mu, int s) const {
+        const double2* b = link(mu, s);
         Rows2<double> a;
 #pragma unroll
         for (int e = 0; e < 6; e++) {
-            const double2 v = __ldg(plane(mu, e) + s);
+            const double2 v = __ldg(b + 32 * e);
             a.e[e / 3][e % 3] = cx(v.x, v.y);
         }
         return a;
     }
     __device__ __forceinline__ M3<double> load(int mu, int s) const {
+        const double2* b = link(mu, s);
         M3<double> a;
 #pragma unroll
         for (int e = 0; e < NE; e++) {
-            const double2 v = __ldg(plane(mu, e) + s);
+            const double2 v = __ldg(b + 32 * e);
             set_elem(a, e, v.x, v.y);
         }
         if (NE == 6) reconstruct_row2(a);
         return a;
     }
     __device__ __forceinline__ void put(int mu, int e, int s, Cx<double> v) const {
-        double2* q = const_cast<double2*>(plane(mu, e)) + s;
+        double2* q = const_cast<double2*>(link(mu, s)) + 32 * e;
         *q = make_double2(v.re, v.im);
     }
     __device__ __forceinline__ void store(int mu, int s, const M3<double>& a) const {
+        double2* q = const_cast<double2*>(link(mu, s));
 #pragma unroll
-        for (int e = 0; e < NE; e++) put(mu, e, s, a.e[e / 3][e % 3]);
+        for (int e = 0; e < NE; e++) q[32 * e] = make_double2(a.e[e / 3][e % 3].re, a.e[e / 3][e % 3].im);
     }
     __device__ __forceinline__ void store_rows2(int mu, int s, const Rows2<double>& a) const {
+        double2* q = const_cast<double2*>(link(mu, s));
 #pragma unroll
-        for (int e = 0; e < 6; e++) put(mu, e, s, a.e[e / 3][e % 3]);
+        for (int e = 0; e < 6; e++) q[32 * e] = make_double2(a.e[e / 3][e % 3].re, a.e[e / 3][e % 3].im);
         if (NE == 9) {
 #pragma unroll
-            for (int k = 0; k < 3; k++) put(mu, 6 + k, s, row2_entry(a, k));
+            for (int k = 0; k < 3; k++) {
+                const Cx<double> r = row2_entry(a, k);
+                q[32 * (6 + k)] = make_double2(r.re, r.im);
+            }
         }
     }
 };
@@ -158,62 +183,65 @@ template <int NE>
 struct LinkField<float, NE> {
     using Real = float;
     static constexpr int kElems = NE;
-    static constexpr int kPairs = NE / 2;  // float4 planes per mu: 3 (12-real) or 4 (18-real)
+    static constexpr int kPairs = NE / 2;                        // float4 blocks: 3 (12-real) or 4 (18-real)
+    static constexpr int kUnits = kPairs * 32 + (NE == 9 ? 16 : 0);  // + the float2 block of element 8
     void* p;
     int V;
 
-    __device__ __forceinline__ const float4* pair(int mu, int k) const {
-        return reinterpret_cast<const float4*>(p) + int64_t(mu * kPairs + k) * V;
+    // pair 0 of link (mu, s); pair k is 32 units further per k
+    __device__ __forceinline__ const float4* link(int mu, int s) const {
+        return reinterpret_cast<const float4*>(p) + group_lane_unit(mu, s, V, kUnits);
     }
-    // element 8 of the 18-real form, after all float4 planes
-    __device__ __forceinline__ const float2* tail(int mu) const {
-        return reinterpret_cast<const float2*>(reinterpret_cast<const float4*>(p) + int64_t(4 * kPairs) * V) +
-               int64_t(mu) * V;
+    // element 8 of the 18-real form: the float2 block after the float4 blocks
+    __device__ __forceinline__ const float2* tail(const float4* l, int s) const {
+        return reinterpret_cast<const float2*>(l - (s & 31) + 32 * kPairs) + (s & 31);
     }
     __device__ __forceinline__ Rows2<float> load_rows2(int mu, int s) const {
+        const float4* b = link(mu, s);
         Rows2<float> a;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const float4 v = __ldg(pair(mu, k) + s);
+            const float4 v = __ldg(b + 32 * k);
             a.e[(2 * k) / 3][(2 * k) % 3] = cx(v.x, v.y);
             a.e[(2 * k + 1) / 3][(2 * k + 1) % 3] = cx(v.z, v.w);
         }
         return a;
     }
     __device__ __forceinline__ M3<float> load(int mu, int s) const {
+        const float4* b = link(mu, s);
         M3<float> a;
 #pragma unroll
         for (int k = 0; k < kPairs; k++) {
-            const float4 v = __ldg(pair(mu, k) + s);
+            const float4 v = __ldg(b + 32 * k);
             set_elem(a, 2 * k, v.x, v.y);
             set_elem(a, 2 * k + 1, v.z, v.w);
         }
         if (NE == 9) {
-            const float2 v = __ldg(tail(mu) + s);
+            const float2 v = __ldg(tail(b, s));
             set_elem(a, 8, v.x, v.y);
         } else {
             reconstruct_row2(a);
         }
         return a;
     }
-    __device__ __forceinline__ void put_pair(int mu, int k, int s, Cx<float> x, Cx<float> y) const {
-        float4* q = const_cast<float4*>(pair(mu, k)) + s;
-        *q = make_float4(x.re, x.im, y.re, y.im);
-    }
     __device__ __forceinline__ void store(int mu, int s, const M3<float>& a) const {
+        float4* q = const_cast<float4*>(link(mu, s));
 #pragma unroll
-        for (int k = 0; k < kPairs; k++)
-            put_pair(mu, k, s, a.e[(2 * k) / 3][(2 * k) % 3], a.e[(2 * k + 1) / 3][(2 * k + 1) % 3]);
-        if (NE == 9) *(const_cast<float2*>(tail(mu)) + s) = make_float2(a.e[2][2].re, a.e[2][2].im);
+        for (int k = 0; k < kPairs; k++) {
+            const Cx<float> x = a.e[(2 * k) / 3][(2 * k) % 3], y = a.e[(2 * k + 1) / 3][(2 * k + 1) % 3];
+            q[32 * k] = make_float4(x.re, x.im, y.re, y.im);
+        }
+        if (NE == 9) *const_cast<float2*>(tail(q, s)) = make_float2(a.e[2][2].re, a.e[2][2].im);
     }
     __device__ __forceinline__ void store_rows2(int mu, int s, const Rows2<float>& a) const {
-        put_pair(mu, 0, s, a.e[0][0], a.e[0][1]);
-        put_pair(mu, 1, s, a.e[0][2], a.e[1][0]);
-        put_pair(mu, 2, s, a.e[1][1], a.e[1][2]);
+        float4* q = const_cast<float4*>(link(mu, s));
+        q[0] = make_float4(a.e[0][0].re, a.e[0][0].im, a.e[0][1].re, a.e[0][1].im);
+        q[32] = make_float4(a.e[0][2].re, a.e[0][2].im, a.e[1][0].re, a.e[1][0].im);
+        q[64] = make_float4(a.e[1][1].re, a.e[1][1].im, a.e[1][2].re, a.e[1][2].im);
         if (NE == 9) {
             const Cx<float> r0 = row2_entry(a, 0), r1 = row2_entry(a, 1), r2 = row2_entry(a, 2);
-            put_pair(mu, 3, s, r0, r1);
-            *(const_cast<float2*>(tail(mu)) + s) = make_float2(r2.re, r2.im);
+            q[96] = make_float4(r0.re, r0.im, r1.re, r1.im);
+            *const_cast<float2*>(tail(q, s)) = make_float2(r2.re, r2.im);
         }
     }
 };
@@ -227,13 +255,14 @@ struct ForceField;
 
 template <>
 struct ForceField<double> {
-    void* p;  // 4 double2 planes per mu
+    void* p;  // 4 double2 blocks per (mu, group)
     int V;
-    __device__ __forceinline__ double2* plane(int mu, int k) const {
-        return reinterpret_cast<double2*>(p) + int64_t(mu * 4 + k) * V;
+    __device__ __forceinline__ double2* link(int mu, int s) const {
+        return reinterpret_cast<double2*>(p) + group_lane_unit(mu, s, V, 4 * 32);
     }
     __device__ __forceinline__ Herm8<double> load(int mu, int s) const {
-        const double2 a = plane(mu, 0)[s], b = plane(mu, 1)[s], c = plane(mu, 2)[s], d = plane(mu, 3)[s];
+        const double2* q = link(mu, s);
+        const double2 a = q[0], b = q[32], c = q[64], d = q[96];
         Herm8<double> z;
         z.d0 = a.x;
         z.d1 = a.y;
@@ -243,22 +272,24 @@ struct ForceField<double> {
         return z;
     }
     __device__ __forceinline__ void store(int mu, int s, const Herm8<double>& z) const {
-        plane(mu, 0)[s] = make_double2(z.d0, z.d1);
-        plane(mu, 1)[s] = make_double2(z.z01.re, z.z01.im);
-        plane(mu, 2)[s] = make_double2(z.z02.re, z.z02.im);
-        plane(mu, 3)[s] = make_double2(z.z12.re, z.z12.im);
+        double2* q = link(mu, s);
+        q[0] = make_double2(z.d0, z.d1);
+        q[32] = make_double2(z.z01.re, z.z01.im);
+        q[64] = make_double2(z.z02.re, z.z02.im);
+        q[96] = make_double2(z.z12.re, z.z12.im);
     }
 };
 
 template <>
 struct ForceField<float> {
-    void* p;  // 2 float4 planes per mu
+    void* p;  // 2 float4 blocks per (mu, group)
     int V;
-    __device__ __forceinline__ float4* plane(int mu, int k) const {
-        return reinterpret_cast<float4*>(p) + int64_t(mu * 2 + k) * V;
+    __device__ __forceinline__ float4* link(int mu, int s) const {
+        return reinterpret_cast<float4*>(p) + group_lane_unit(mu, s, V, 2 * 32);
     }
     __device__ __forceinline__ Herm8<float> load(int mu, int s) const {
-        const float4 a = plane(mu, 0)[s], b = plane(mu, 1)[s];
+        const float4* q = link(mu, s);
+        const float4 a = q[0], b = q[32];
         Herm8<float> z;
         z.d0 = a.x;
         z.d1 = a.y;
@@ -268,8 +299,9 @@ struct ForceField<float> {
         return z;
     }
     __device__ __forceinline__ void store(int mu, int s, const Herm8<float>& z) const {
-        plane(mu, 0)[s] = make_float4(z.d0, z.d1, z.z01.re, z.z01.im);
-        plane(mu, 1)[s] = make_float4(z.z02.re, z.z02.im, z.z12.re, z.z12.im);
+        float4* q = link(mu, s);
+        q[0] = make_float4(z.d0, z.d1, z.z01.re, z.z01.im);
+        q[32] = make_float4(z.z02.re, z.z02.im, z.z12.re, z.z12.im);
     }
 };
 

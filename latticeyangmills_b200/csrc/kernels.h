@@ -15,6 +15,11 @@ enum Precision { kFP64 = 0, kFP32_18 = 1, kFP32_12 = 2 };
 inline int link_elems(int prec) { return prec == kFP32_12 ? 6 : 9; }
 inline size_t link_bytes(int prec) { return prec == kFP64 ? 9 * 16 : size_t(link_elems(prec)) * 8; }
 inline size_t force_bytes(int prec) { return prec == kFP64 ? 64 : 32; }
+// device bytes of a link field / a generator field (volume padded to whole warp groups)
+inline size_t link_field_bytes(int prec, int64_t V) { return size_t(4 * padded_sites(V)) * link_bytes(prec); }
+inline size_t force_field_bytes(int prec, int64_t V) { return size_t(4 * padded_sites(V)) * force_bytes(prec); }
+// whether field.cuh's 32-bit offsets (16-byte units) reach every link of V sites
+inline bool volume_addressable(int prec, int64_t V) { return link_field_bytes(prec, V) / 16 < (size_t(1) << 32); }
 
 // One RK3 stage (0, 1, 2) over every link: staples, generator, RK combination
 // with the stored generator, e^{i eps_stage Z} and the link update uin -> uout.

@@ -240,12 +240,12 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
         }
         V *= dims[i];
     }
-    if (V >= (int64_t(1) << 31)) {
-        set(YMFLOW_ERR_ARG, "lattice volume must be below 2^31 sites");
-        return nullptr;
-    }
     if (precision < YMFLOW_FP64 || precision > YMFLOW_FP32_12) {
         set(YMFLOW_ERR_ARG, "unknown precision");
+        return nullptr;
+    }
+    if (V >= (int64_t(1) << 31) || !volume_addressable(precision, V)) {
+        set(YMFLOW_ERR_ARG, "lattice volume too large (4 V link bytes must stay below 64 GiB)");
         return nullptr;
     }
     std::string why;
@@ -265,8 +265,8 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     c->geo = make_geo(dims);
     int r = YMFLOW_OK;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) r = YMFLOW_ERR_CUDA;
-    const size_t ub = size_t(4 * V) * link_bytes(c->prec);
-    const size_t zb = size_t(4 * V) * force_bytes(c->prec);
+    const size_t ub = link_field_bytes(c->prec, V);
+    const size_t zb = force_field_bytes(c->prec, V);
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[0], ub, "link buffer 0");
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[1], ub, "link buffer 1");
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->z, zb, "force buffer");
