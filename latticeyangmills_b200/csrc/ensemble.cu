@@ -44,7 +44,7 @@ __device__ __forceinline__ int find_conf(const EnsConf* confs, int nconf, int it
 
 template <class F>
 struct EnsMinBlocks {
-    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : 5;
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : 5;  // the persistent loop spills at 80 registers
 };
 
 template <class F, int STAGE>
