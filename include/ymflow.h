@@ -187,6 +187,48 @@ YMFLOW_API int ymflow_time_steps(ymflow_ctx* ctx, double eps, int nsteps, float*
 YMFLOW_API int ymflow_set_option(ymflow_ctx* ctx, int key, int64_t value);
 YMFLOW_API int ymflow_get_option(const ymflow_ctx* ctx, int key, int64_t* value);
 
+/* --- One configuration split along t over several GPUs -------------------- */
+/* A slab context holds the time slices [t0, t0 + nt) of a configuration of
+ * extents global_dims on one GPU, with one halo slice on each side.  It
+ * replaces the reference's MPI domain decomposition
+ * (src/ParallelTools/parallel.cpp:57-100, "SubLatticeSize") for the time
+ * direction.  The spatial volume x y z must be a multiple of 32.
+ * ymflow_upload/_download/_upload_sites/_download_sites address the slab's own
+ * sites, which are sites [t0 Vs, (t0 + nt) Vs) of the .bin file (Vs = x y z).
+ * ymflow_init_links draws the same links as a whole-lattice context with the
+ * same seed.  Observables are of the whole configuration once summed over the
+ * slabs.  ymflow_derivative and ymflow_generate_metropolis need a whole-lattice
+ * context.
+ *
+ * A slab flows in one of two ways:
+ *  - one process per GPU: ymflow_slab_connect, then ymflow_flow /
+ *    ymflow_observables / ymflow_time_steps as usual.  These become collective
+ *    over the ranks (every rank calls them with the same arguments).  Halos
+ *    travel by NCCL send/recv after every stage; measurement rows are summed
+ *    with an NCCL all-reduce.  NCCL (libnccl.so.2) is loaded at run time;
+ *    YMFLOW_ERR_NODEVICE if it is missing.
+ *  - several slabs in one process (one or more GPUs): ymflow_slab_group_flow,
+ *    with halos as stream-ordered peer copies.
+ * A slab that is neither connected nor flowed through its group returns
+ * YMFLOW_ERR_STATE from ymflow_flow. */
+YMFLOW_API ymflow_ctx* ymflow_create_slab(const int global_dims[4], int t0, int nt, int precision, int device,
+                                          int* status);
+
+/* NCCL communicator set-up: rank 0 makes the id and shares its bytes with the
+ * other ranks (e.g. through torch.distributed); every rank then connects its
+ * slab, naming the ranks that hold the slices below t0 and above t0 + nt - 1
+ * (periodically; a single rank is its own neighbour). */
+#define YMFLOW_NCCL_ID_BYTES 128
+YMFLOW_API int ymflow_nccl_unique_id(void* id);
+YMFLOW_API int ymflow_slab_connect(ymflow_ctx* ctx, const void* id, int rank, int nranks, int lower_rank,
+                                   int upper_rank);
+
+/* ymflow_flow over the n slab contexts of one configuration, in time order
+ * (ctxs[i] starts where ctxs[i-1] ends), held in this process.  Rows as
+ * ymflow_flow's, for the whole configuration. */
+YMFLOW_API int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nsteps, int measure_every,
+                                      int reunit_every, ymflow_obs* out, int out_cap, int* n_out);
+
 /* Measured CUDA-core FMA throughput of `device` in TFLOP/s (2 flops per FMA):
  * FP64 FMAs for YMFLOW_FP64, FP32 FMAs otherwise.  A measurement utility with
  * no counterpart in the reference: the denominator of the stage kernels'

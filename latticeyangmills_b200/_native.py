@@ -28,6 +28,7 @@ FP64, FP32_18, FP32_12 = 0, 1, 2
 PRECISIONS = {"fp64": FP64, "fp32_18": FP32_18, "fp32_12": FP32_12}
 FIELD_COLD, FIELD_EXPIAH, FIELD_HOT, FIELD_CURRENT = 0, 1, 2, 3
 IO_BIG_ENDIAN = 1
+NCCL_ID_BYTES = 128
 OPT_BLOCK, OPT_GRAPH, OPT_OBS_BLOCK = 1, 2, 3
 
 # every symbol include/ymflow.h declares
@@ -41,8 +42,10 @@ EXPORTS = (
     "ymflow_ensemble_upload", "ymflow_ensemble_download", "ymflow_ensemble_init_links",
     "ymflow_ensemble_flow", "ymflow_ensemble_reset_time", "ymflow_ensemble_time_steps",
     "ymflow_ensemble_autotune", "ymflow_observables_noalloc",
+    "ymflow_create_slab", "ymflow_nccl_unique_id", "ymflow_slab_connect", "ymflow_slab_group_flow",
 )
-NON_INT = ("ymflow_version", "ymflow_create", "ymflow_destroy", "ymflow_last_error", "ymflow_ensemble_create",
+NON_INT = ("ymflow_version", "ymflow_create", "ymflow_create_slab", "ymflow_destroy", "ymflow_last_error",
+           "ymflow_ensemble_create",
            "ymflow_ensemble_destroy", "ymflow_ensemble_last_error")
 
 
@@ -126,6 +129,12 @@ def load():
     l.ymflow_ensemble_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     l.ymflow_ensemble_autotune.argtypes = [vp, ctypes.c_double, IP, IP]
     l.ymflow_observables_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_int), vp, vp]
+    l.ymflow_create_slab.argtypes = [IP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, IP]
+    l.ymflow_create_slab.restype = vp
+    l.ymflow_nccl_unique_id.argtypes = [vp]
+    l.ymflow_slab_connect.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    l.ymflow_slab_group_flow.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(Obs), ctypes.c_int, IP]
     for name in EXPORTS:
         if name not in NON_INT:
             getattr(l, name).restype = ctypes.c_int

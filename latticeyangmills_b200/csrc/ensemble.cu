@@ -370,9 +370,8 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->confs_dev, sizeof(EnsConf) * nconf, "work list");
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->deviation, sizeof(unsigned long long), "drift flag");
     if (r == YMFLOW_OK) {
-        Geo gmax{};
-        gmax.V = e->max_v;
-        e->partial_cap = std::max(obs_blocks(gmax, 32), 1);
+        // most observable blocks of any configuration: the largest one at the smallest block (32)
+        e->partial_cap = std::max(int((e->max_v + 31) / 32), 1);
         r = ens_alloc(e, (void**)&e->partials, size_t(e->partial_cap) * 3 * sizeof(double), "partials");
     }
     if (r == YMFLOW_OK && (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess))

@@ -55,6 +55,13 @@ struct Geo {
     int stride[4];  // 1, nx, nx*ny, nx*ny*nz
     int V;
     FastDiv div[3];  // by n[0], n[1], n[2]
+    // Sites this context updates and measures, [site0, site1): the whole
+    // lattice, or the interior time slices of a slab of a decomposed
+    // configuration (whose first and last slices are halos).  global0 is the
+    // configuration-wide site index of site0 (seeded fields use global link
+    // indices), vglobal the configuration's volume (normalisations).
+    int site0, site1;
+    long long global0, vglobal;
 
     __device__ __forceinline__ static int fdiv(int x, const FastDiv& f) {
         return int((uint64_t(uint32_t(x)) * f.m) >> (32 + f.l));
@@ -102,6 +109,10 @@ inline Geo make_geo(const int dims[4]) {
     g.stride[3] = dims[0] * dims[1] * dims[2];
     g.V = dims[0] * dims[1] * dims[2] * dims[3];
     for (int i = 0; i < 3; i++) g.div[i] = make_fastdiv(dims[i]);
+    g.site0 = 0;
+    g.site1 = g.V;
+    g.global0 = 0;
+    g.vglobal = g.V;
     return g;
 }
 

@@ -129,12 +129,16 @@ __device__ __forceinline__ double2 gauss2(uint64_t seed, uint32_t config, uint64
     return make_double2(r * cp, r * sp);
 }
 
+// Links of the sites [g.site0, g.site1); the random numbers of a link are drawn
+// by its configuration-wide index (l below), so a slab of a decomposed
+// configuration holds the same links as the whole-lattice field.
 template <class F>
-__global__ void init_kernel(F u, int V, int kind, double a, uint64_t seed, uint32_t config) {
-    const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * int64_t(V)) return;
-    const int s = int(l >> 2);
-    const int mu = int(l & 3);
+__global__ void init_kernel(F u, Geo g, int kind, double a, uint64_t seed, uint32_t config) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= 4 * int64_t(g.site1 - g.site0)) return;
+    const int s = g.site0 + int(k >> 2);
+    const int mu = int(k & 3);
+    const int64_t l = 4 * g.global0 + k;
     using R = typename F::Real;
     M3<double> m;
     if (kind == kCold) {
@@ -200,9 +204,10 @@ __device__ __forceinline__ void gram_schmidt(M3<double>& m) {
 }
 
 template <class F>
-__global__ void haar_kernel(F u, int V, double frac, uint64_t seed, uint32_t config) {
-    const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (l >= 4 * int64_t(V)) return;
+__global__ void haar_kernel(F u, Geo g, double frac, uint64_t seed, uint32_t config) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= 4 * int64_t(g.site1 - g.site0)) return;
+    const int64_t l = 4 * g.global0 + k;
     const uint4 o = philox4x32(make_uint4(uint32_t(l), uint32_t(uint64_t(l) >> 32), config, uint32_t(kStreamPick) << 16),
                                make_uint2(uint32_t(seed), uint32_t(seed >> 32)));
     if (!(u53(o.x, o.y) < frac)) return;
@@ -219,17 +224,18 @@ __global__ void haar_kernel(F u, int V, double frac, uint64_t seed, uint32_t con
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) r.e[i][j] = cx(R(m.e[i][j].re), R(m.e[i][j].im));
-    u.store(int(l & 3), int(l >> 2), r);
+    u.store(int(k & 3), g.site0 + int(k >> 2), r);
 }
 
 cudaError_t launch_init_links(int prec, void* u, const Geo& g, int kind, double a, uint64_t seed, uint32_t config,
                               cudaStream_t st) {
     const int b = 128;
-    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
+    const unsigned nb = unsigned((4 * int64_t(g.site1 - g.site0) + b - 1) / b);
+    if (nb == 0) return cudaSuccess;
     switch (prec) {
-        case kFP64: init_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, g.V, kind, a, seed, config); break;
-        case kFP32_18: init_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, g.V, kind, a, seed, config); break;
-        case kFP32_12: init_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, g.V, kind, a, seed, config); break;
+        case kFP64: init_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, g, kind, a, seed, config); break;
+        case kFP32_18: init_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, g, kind, a, seed, config); break;
+        case kFP32_12: init_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, g, kind, a, seed, config); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -238,11 +244,12 @@ cudaError_t launch_init_links(int prec, void* u, const Geo& g, int kind, double 
 cudaError_t launch_haar_mix(int prec, void* u, const Geo& g, double frac, uint64_t seed, uint32_t config,
                             cudaStream_t st) {
     const int b = 128;
-    const unsigned nb = unsigned((4 * g.V + b - 1) / b);
+    const unsigned nb = unsigned((4 * int64_t(g.site1 - g.site0) + b - 1) / b);
+    if (nb == 0) return cudaSuccess;
     switch (prec) {
-        case kFP64: haar_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, g.V, frac, seed, config); break;
-        case kFP32_18: haar_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, g.V, frac, seed, config); break;
-        case kFP32_12: haar_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, g.V, frac, seed, config); break;
+        case kFP64: haar_kernel<<<nb, b, 0, st>>>(FieldD18{const_cast<void*>((const void*)u), g.V}, g, frac, seed, config); break;
+        case kFP32_18: haar_kernel<<<nb, b, 0, st>>>(FieldF18{const_cast<void*>((const void*)u), g.V}, g, frac, seed, config); break;
+        case kFP32_12: haar_kernel<<<nb, b, 0, st>>>(FieldF12{const_cast<void*>((const void*)u), g.V}, g, frac, seed, config); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -10,10 +10,10 @@ namespace ym {
 // mu = w & 3 for 32 consecutive sites, so the four directions of a site range
 // run side by side and share their neighbour links through L1/L2 (a grid that
 // sweeps all sites once per direction streams the field through L2 four times).
-__device__ __forceinline__ void link_of_thread(int& s, int& mu) {
+__device__ __forceinline__ void link_of_thread(const Geo& g, int& s, int& mu) {
     const int w = threadIdx.x >> 5;
     mu = w & 3;
-    s = int(blockIdx.x) * (blockDim.x >> 2) + ((w >> 2) << 5) + (threadIdx.x & 31);
+    s = g.site0 + int(blockIdx.x) * (blockDim.x >> 2) + ((w >> 2) << 5) + (threadIdx.x & 31);
 }
 
 // Resident 128-thread blocks per SM the stage kernel is compiled for (caps its
@@ -31,8 +31,8 @@ __global__ void __launch_bounds__(128, StageMinBlocks<F>::value)
     rk_stage_kernel(F in, F out, ForceField<typename F::Real> zf, Geo g, typename F::Real eps) {
     int s;
     int mu;
-    link_of_thread(s, mu);
-    if (s >= g.V) return;
+    link_of_thread(g, s, mu);
+    if (s >= g.site1) return;
     rk_link_update<F, STAGE>(in, out, zf, g, eps, s, mu);
 }
 
@@ -43,7 +43,7 @@ static cudaError_t launch_typed(int stage, const void* uin, void* uout, void* z,
     F in{const_cast<void*>(uin), g.V}, out{uout, g.V};
     ForceField<R> zf{z, g.V};
     const int sites_per_block = block / 4;
-    dim3 grid(unsigned((g.V + sites_per_block - 1) / sites_per_block));
+    dim3 grid(unsigned((g.site1 - g.site0 + sites_per_block - 1) / sites_per_block));
     const R e = R(stage == 0 ? eps * 0.25 : eps);
     switch (stage) {
         case 0: rk_stage_kernel<F, 0><<<grid, block, 0, st>>>(in, out, zf, g, e); break;

@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(1024) obs_finalize_kernel(const double* partia
     }
 }
 
-int obs_blocks(const Geo& g, int block) { return int((g.V + block - 1) / block); }
+int obs_blocks(const Geo& g, int block) { return int((g.site1 - g.site0 + block - 1) / block); }
 
 cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* partials, int block, cudaStream_t st) {
     const unsigned nb = unsigned(obs_blocks(g, block));
@@ -64,7 +64,7 @@ cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* pa
 }
 
 cudaError_t launch_obs_finalize(const double* partials, int nblocks, const Geo& g, double* out, cudaStream_t st) {
-    obs_finalize_kernel<<<1, 1024, 0, st>>>(partials, nblocks, 1.0 / (18.0 * double(g.V)), out);
+    obs_finalize_kernel<<<1, 1024, 0, st>>>(partials, nblocks, 1.0 / (18.0 * double(g.vglobal)), out);
     return cudaGetLastError();
 }
 

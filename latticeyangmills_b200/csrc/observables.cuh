@@ -164,9 +164,9 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c) {
 
 template <class F>
 __global__ void __launch_bounds__(256) observables_kernel(F u, Geo g, double* partials) {
-    const int s = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int s = g.site0 + int(blockIdx.x) * blockDim.x + threadIdx.x;
     double plaq = 0.0, energy = 0.0, topc = 0.0;
-    if (s < g.V) site_observables(u, g, s, plaq, energy, topc);
+    if (s < g.site1) site_observables(u, g, s, plaq, energy, topc);
     block_sum3(plaq, energy, topc);
     if (threadIdx.x == 0) {
         partials[3 * blockIdx.x + 0] = plaq;

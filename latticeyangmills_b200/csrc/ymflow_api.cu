@@ -11,48 +11,12 @@
 #include <string>
 #include <vector>
 
-#include "api_util.h"
-#include "kernels.h"
-#include "ymflow.h"
+#include "context.h"
 
 using namespace ym;
 
-struct ymflow_ctx {
-    int dims[4] = {0, 0, 0, 0};
-    int prec = 0;
-    int device = 0;
-    Geo geo{};
-    cudaStream_t stream = nullptr;
-    void* u[2] = {nullptr, nullptr};  // ping-pong link buffers
-    int cur = 0;                      // which of u[] holds the current field
-    void* z = nullptr;                // RK generator, 8 reals per link
-    double* staging = nullptr;        // .bin-layout device buffer for upload/download
-    size_t staging_bytes = 0;
-    double* partials = nullptr;       // observables: 3 doubles per block
-    int partial_cap = 0;
-    double* meas = nullptr;           // measurement rows on the device, 4 doubles each
-    int meas_cap = 0;
-    double* meas_host = nullptr;      // pinned copy of the rows
-    unsigned long long* deviation = nullptr;  // reunitarisation drift (ordered bits)
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    double graph_eps[2] = {0.0, 0.0};
-    int graph_block[2] = {0, 0};
-    std::vector<cudaEvent_t> events;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int block = 128;
-    int obs_block = 128;
-    bool use_graph = true;
-    bool loaded = false;
-    int64_t step = 0;
-    double t = 0.0;
-    uint32_t gen_sweep = 0;           // Metropolis sweeps since the last cold/hot start
-    int64_t bytes = 0;
-    std::string err;
-};
 
-namespace {
-
-thread_local std::string g_create_error;
+namespace ym {
 
 int fail(ymflow_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -61,11 +25,11 @@ int fail(ymflow_ctx* c, int code, const std::string& msg) {
 
 int cuda_fail(ymflow_ctx* c, cudaError_t e, const char* what) { return fail(c, status_of(e), cuda_message(e, what)); }
 
-#define YM_CK(ctx, call, what)                               \
-    do {                                                     \
-        cudaError_t e_ = (call);                             \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
-    } while (0)
+}  // namespace ym
+
+namespace {
+
+thread_local std::string g_create_error;
 
 int64_t link_count(const ymflow_ctx* c) { return 4 * c->geo.V; }
 
@@ -108,6 +72,10 @@ int ensure_partials(ymflow_ctx* c) {
     return r;
 }
 
+}  // namespace
+
+namespace ym {
+
 int ensure_meas(ymflow_ctx* c, int rows) {
     if (rows <= c->meas_cap) return YMFLOW_OK;
     if (c->meas) {
@@ -127,6 +95,10 @@ int ensure_meas(ymflow_ctx* c, int rows) {
     c->meas_cap = rows;
     return YMFLOW_OK;
 }
+
+}  // namespace ym
+
+namespace {
 
 void drop_graphs(ymflow_ctx* c) {
     for (int i = 0; i < 2; i++) {
@@ -150,7 +122,25 @@ cudaError_t enqueue_step(ymflow_ctx* c, int from, double eps, cudaEvent_t* ev) {
     return cudaSuccess;
 }
 
+// One RK3 step of a slab: each stage's new links are followed by the halo
+// exchange of that buffer, which the next stage reads.
+int run_step_slab(ymflow_ctx* c, double eps, cudaEvent_t* ev) {
+    const int from = c->cur;
+    const int in[3] = {from, 1 - from, from};
+    for (int s = 0; s < 3; s++) {
+        if (ev) cudaEventRecord(ev[2 * s], c->stream);
+        YM_CK(c, launch_rk_stage(c->prec, s, c->u[in[s]], c->u[1 - in[s]], c->z, c->geo, eps, c->block, c->stream),
+              "stage launch");
+        if (ev) cudaEventRecord(ev[2 * s + 1], c->stream);
+        const int r = slab_exchange(c, 1 - in[s]);
+        if (r != YMFLOW_OK) return r;
+    }
+    c->cur = 1 - from;
+    return YMFLOW_OK;
+}
+
 int run_step(ymflow_ctx* c, double eps, cudaEvent_t* ev) {
+    if (c->slab) return run_step_slab(c, eps, ev);
     const int from = c->cur;
     if (c->use_graph && !ev) {
         if (!c->graph[from] || c->graph_eps[from] != eps || c->graph_block[from] != c->block) {
@@ -179,6 +169,10 @@ int run_step(ymflow_ctx* c, double eps, cudaEvent_t* ev) {
     return YMFLOW_OK;
 }
 
+}  // namespace
+
+namespace ym {
+
 // Observables of the current field into meas row `row` (device).
 int enqueue_measure(ymflow_ctx* c, int row) {
     int r = ensure_partials(c);
@@ -187,8 +181,10 @@ int enqueue_measure(ymflow_ctx* c, int row) {
           "observables launch");
     YM_CK(c, launch_obs_finalize(c->partials, obs_blocks(c->geo, c->obs_block), c->geo, c->meas + 4 * row, c->stream),
           "observables fold");
+    if (c->slab && c->comm) return slab_reduce_row(c, c->meas + 4 * row);
     return YMFLOW_OK;
 }
+
 
 void fill_obs(const ymflow_ctx* c, const double* m, int64_t step, double t, ymflow_obs* o) {
     o->step = int32_t(step);
@@ -197,10 +193,21 @@ void fill_obs(const ymflow_ctx* c, const double* m, int64_t step, double t, ymfl
     o->plaq = m[0];
     o->topc = m[1];
     o->energy = m[2];
-    o->t2E = -t * t * m[2] / (64.0 * double(c->geo.V));
+    o->t2E = -t * t * m[2] / (64.0 * double(c->geo.vglobal));
 }
 
-}  // namespace
+// A slab measures and flows only once connected; its halos are refreshed from
+// the neighbours first (the field may have been uploaded or initialised since).
+int slab_prepare(ymflow_ctx* c) {
+    if (!c->slab) return YMFLOW_OK;
+    if (!c->comm)
+        return fail(c, YMFLOW_ERR_STATE,
+                    "slab context not connected: call ymflow_slab_connect, or flow its group with "
+                    "ymflow_slab_group_flow");
+    return slab_exchange(c, c->cur);
+}
+
+}  // namespace ym
 
 extern "C" {
 
@@ -284,10 +291,53 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     return c;
 }
 
+ymflow_ctx* ymflow_create_slab(const int global_dims[4], int t0, int nt, int precision, int device, int* status) {
+    auto set = [&](int s, const std::string& m) {
+        if (status) *status = s;
+        g_create_error = m;
+    };
+    if (!global_dims) {
+        set(YMFLOW_ERR_ARG, "global_dims is NULL");
+        return nullptr;
+    }
+    for (int i = 0; i < 4; i++)
+        if (global_dims[i] < 1 || global_dims[i] > 4096) {
+            set(YMFLOW_ERR_ARG, "lattice extents must be in 1..4096");
+            return nullptr;
+        }
+    if (nt < 1 || t0 < 0 || int64_t(t0) + nt > global_dims[3] || nt + 2 > 4096) {
+        set(YMFLOW_ERR_ARG, "slab slices [t0, t0 + nt) outside the lattice's time extent");
+        return nullptr;
+    }
+    const int64_t vs = int64_t(global_dims[0]) * global_dims[1] * global_dims[2];
+    if (vs % 32 != 0) {
+        set(YMFLOW_ERR_ARG, "a slab needs a spatial volume (x y z) divisible by 32");
+        return nullptr;
+    }
+    if (vs * global_dims[3] >= (int64_t(1) << 31)) {
+        set(YMFLOW_ERR_ARG, "lattice volume must be below 2^31 sites");
+        return nullptr;
+    }
+    const int local[4] = {global_dims[0], global_dims[1], global_dims[2], nt + 2};
+    ymflow_ctx* c = ymflow_create(local, precision, device, status);
+    if (!c) return nullptr;
+    c->slab = true;
+    c->t0 = t0;
+    c->nt = nt;
+    for (int i = 0; i < 4; i++) c->gdims[i] = global_dims[i];
+    c->geo.site0 = int(vs);
+    c->geo.site1 = int(vs * (nt + 1));
+    c->geo.global0 = int64_t(t0) * vs;
+    c->geo.vglobal = vs * global_dims[3];
+    c->use_graph = false;
+    return c;
+}
+
 void ymflow_destroy(ymflow_ctx* c) {
     if (!c) return;
     DeviceGuard guard(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    slab_release(c);
     drop_graphs(c);
     for (void* p : {c->u[0], c->u[1], c->z, (void*)c->staging, (void*)c->partials, (void*)c->meas,
                     (void*)c->deviation})
@@ -307,30 +357,12 @@ const char* ymflow_last_error(const ymflow_ctx* c) {
 
 int ymflow_upload(ymflow_ctx* c, const double* links) {
     if (!c || !links) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_upload");
-    DeviceGuard guard(c->device);
-    int r = ensure_staging(c);
-    if (r != YMFLOW_OK) return r;
-    const size_t bytes = size_t(link_count(c)) * 18 * sizeof(double);
-    YM_CK(c, cudaMemcpyAsync(c->staging, links, bytes, cudaMemcpyHostToDevice, c->stream), "upload copy");
-    YM_CK(c, launch_pack(c->prec, c->staging, c->u[c->cur], c->geo, c->stream), "pack launch");
-    YM_CK(c, cudaStreamSynchronize(c->stream), "upload");
-    c->loaded = true;
-    c->step = 0;
-    c->t = 0.0;
-    return YMFLOW_OK;
+    return ymflow_upload_sites(c, links, 0, int64_t(c->geo.site1 - c->geo.site0), 0);
 }
 
 int ymflow_download(ymflow_ctx* c, double* links) {
     if (!c || !links) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_download");
-    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
-    DeviceGuard guard(c->device);
-    int r = ensure_staging(c);
-    if (r != YMFLOW_OK) return r;
-    const size_t bytes = size_t(link_count(c)) * 18 * sizeof(double);
-    YM_CK(c, launch_unpack(c->prec, c->u[c->cur], c->staging, c->geo, c->stream), "unpack launch");
-    YM_CK(c, cudaMemcpyAsync(links, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream), "download copy");
-    YM_CK(c, cudaStreamSynchronize(c->stream), "download");
-    return YMFLOW_OK;
+    return ymflow_download_sites(c, links, 0, int64_t(c->geo.site1 - c->geo.site0), 0);
 }
 
 namespace {
@@ -338,8 +370,8 @@ namespace {
 int check_site_range(ymflow_ctx* c, const void* p, int64_t first, int64_t n, int flags) {
     if (!c) return YMFLOW_ERR_ARG;
     if (!p && n > 0) return fail(c, YMFLOW_ERR_ARG, "null links pointer");
-    if (first < 0 || n < 0 || first + n > int64_t(c->geo.V))
-        return fail(c, YMFLOW_ERR_ARG, "site range outside the lattice");
+    if (first < 0 || n < 0 || first + n > int64_t(c->geo.site1 - c->geo.site0))
+        return fail(c, YMFLOW_ERR_ARG, "site range outside the lattice (or the slab)");
     if (flags & ~YMFLOW_IO_BIG_ENDIAN) return fail(c, YMFLOW_ERR_ARG, "unknown flags");
     return YMFLOW_OK;
 }
@@ -354,7 +386,7 @@ int ymflow_upload_sites(ymflow_ctx* c, const double* links, int64_t first_site, 
     r = ensure_staging(c, bytes);
     if (r != YMFLOW_OK) return r;
     YM_CK(c, cudaMemcpyAsync(c->staging, links, bytes, cudaMemcpyHostToDevice, c->stream), "upload copy");
-    YM_CK(c, launch_pack_range(c->prec, c->staging, c->u[c->cur], c->geo, int(first_site), int(nsites),
+    YM_CK(c, launch_pack_range(c->prec, c->staging, c->u[c->cur], c->geo, c->geo.site0 + int(first_site), int(nsites),
                                (flags & YMFLOW_IO_BIG_ENDIAN) != 0, c->stream),
           "pack launch");
     YM_CK(c, cudaStreamSynchronize(c->stream), "upload");
@@ -373,7 +405,8 @@ int ymflow_download_sites(ymflow_ctx* c, double* links, int64_t first_site, int6
     const size_t bytes = size_t(nsites) * 4 * 18 * sizeof(double);
     r = ensure_staging(c, bytes);
     if (r != YMFLOW_OK) return r;
-    YM_CK(c, launch_unpack_range(c->prec, c->u[c->cur], c->staging, c->geo, int(first_site), int(nsites),
+    YM_CK(c, launch_unpack_range(c->prec, c->u[c->cur], c->staging, c->geo, c->geo.site0 + int(first_site),
+                                 int(nsites),
                                  (flags & YMFLOW_IO_BIG_ENDIAN) != 0, c->stream),
           "unpack launch");
     YM_CK(c, cudaMemcpyAsync(links, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream), "download copy");
@@ -401,6 +434,7 @@ int ymflow_init_links(ymflow_ctx* c, int kind, double a, uint64_t seed, uint32_t
 int ymflow_generate_metropolis(ymflow_ctx* c, int start, double beta, double su3eps, int sweeps, int hits,
                                uint64_t seed, double* acceptance) {
     if (!c) return YMFLOW_ERR_ARG;
+    if (c->slab) return fail(c, YMFLOW_ERR_STATE, "generation runs on a whole-lattice context, not a slab");
     if (sweeps < 0 || hits < 1 || !(su3eps > 0.0 && su3eps < 1.0) || !std::isfinite(beta))
         return fail(c, YMFLOW_ERR_ARG, "need sweeps >= 0, hits >= 1, 0 < su3eps < 1, finite beta");
     if (start != YMFLOW_FIELD_COLD && start != YMFLOW_FIELD_HOT && start != YMFLOW_FIELD_CURRENT)
@@ -443,7 +477,9 @@ int ymflow_observables(ymflow_ctx* c, ymflow_obs* out) {
     if (!c || !out) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_observables");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
     DeviceGuard guard(c->device);
-    int r = enqueue_measure(c, 0);
+    int r = slab_prepare(c);
+    if (r != YMFLOW_OK) return r;
+    r = enqueue_measure(c, 0);
     if (r != YMFLOW_OK) return r;
     YM_CK(c, cudaMemcpyAsync(c->meas_host, c->meas, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
           "observables copy");
@@ -471,6 +507,7 @@ int ymflow_flow(ymflow_ctx* c, double eps, int nsteps, int measure_every, int re
     std::vector<double> row_t(rows);
     const bool reunit = c->prec != YMFLOW_FP64 && reunit_every > 0;
     if (reunit) YM_CK(c, cudaMemsetAsync(c->deviation, 0, sizeof(unsigned long long), c->stream), "reset drift");
+    if ((r = slab_prepare(c)) != YMFLOW_OK) return r;
     int row = 0;
     if ((r = enqueue_measure(c, row)) != YMFLOW_OK) return r;
     row_step[row] = c->step;
@@ -516,6 +553,7 @@ int ymflow_flow(ymflow_ctx* c, double eps, int nsteps, int measure_every, int re
 int ymflow_derivative(ymflow_ctx* c, int mu, double* z_host) {
     if (!c || !z_host || mu < 0 || mu > 3) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_derivative");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    if (c->slab) return fail(c, YMFLOW_ERR_STATE, "ymflow_derivative runs on a whole-lattice context, not a slab");
     DeviceGuard guard(c->device);
     int r = ensure_staging(c);
     if (r != YMFLOW_OK) return r;
@@ -560,6 +598,7 @@ int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, 
     if (!c || !elapsed_ms || nsteps < 1) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_time_steps");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
     DeviceGuard guard(c->device);
+    if (int r = slab_prepare(c)) return r;
     const size_t nev = kernel_ms ? size_t(6) * nsteps : 0;
     while (c->events.size() < nev) {
         cudaEvent_t e;

@@ -85,6 +85,38 @@ class GluonField:
             raise N.YmflowError(st.value, lib.ymflow_last_error(None).decode(errors="replace"))
         self.sites = volume(self.size)
 
+    @classmethod
+    def slab(cls, global_size: Sequence[int], t0: int, nt: int, precision: str = "fp64",
+             device: int = 0) -> "GluonField":
+        """Time slices [t0, t0 + nt) of a configuration of extents global_size,
+        with one halo slice on each side (the reference's domain decomposition,
+        src/ParallelTools/parallel.cpp:57-100, along t).  upload/download and
+        friends address the slab's own sites: the .bin file's sites
+        [t0 Vs, (t0 + nt) Vs).  Flow it with connect() + flow() (one process
+        per GPU) or with slab_group_flow() (all slabs in this process)."""
+        self = cls.__new__(cls)
+        g = tuple(int(v) for v in global_size)
+        self.global_size = g
+        self.t0, self.nt = int(t0), int(nt)
+        self.size = (g[0], g[1], g[2], self.nt)
+        self.precision = precision
+        lib = N.load()
+        st = ctypes.c_int(0)
+        self._ctx = lib.ymflow_create_slab(_dims(g), self.t0, self.nt, N.PRECISIONS[precision], int(device),
+                                           ctypes.byref(st))
+        if not self._ctx:
+            raise N.YmflowError(st.value, lib.ymflow_last_error(None).decode(errors="replace"))
+        self.sites = volume(self.size)
+        return self
+
+    def connect(self, nccl_id: bytes, rank: int, nranks: int, lower: int, upper: int) -> None:
+        """Joins the NCCL communicator of nccl_id (from nccl_unique_id() on rank
+        0); lower/upper are the ranks holding the neighbouring slices."""
+        if len(nccl_id) != N.NCCL_ID_BYTES:
+            raise ValueError("an NCCL id has 128 bytes")
+        buf = ctypes.create_string_buffer(bytes(nccl_id), N.NCCL_ID_BYTES)
+        self._check(N.load().ymflow_slab_connect(self.ctx, buf, int(rank), int(nranks), int(lower), int(upper)))
+
     # lifetime
     def close(self) -> None:
         if getattr(self, "_ctx", None):
@@ -293,6 +325,39 @@ class Ensemble:
 
     def reset_time(self) -> None:
         self._check(N.load().ymflow_ensemble_reset_time(self._ens))
+
+
+def nccl_unique_id() -> bytes:
+    """A fresh NCCL communicator id (128 bytes) for GluonField.connect."""
+    buf = ctypes.create_string_buffer(N.NCCL_ID_BYTES)
+    N.check(N.load().ymflow_nccl_unique_id(buf))
+    return buf.raw
+
+
+def slab_partition(nt_global: int, nranks: int, rank: int):
+    """(t0, nt, lower, upper) of rank's slab when nt_global time slices are
+    split over nranks ranks as evenly as possible, ranks in time order."""
+    if not 1 <= nranks <= nt_global or not 0 <= rank < nranks:
+        raise ValueError("need 1 <= nranks <= time extent and 0 <= rank < nranks")
+    base, extra = divmod(nt_global, nranks)
+    t0 = rank * base + min(rank, extra)
+    nt = base + (1 if rank < extra else 0)
+    return t0, nt, (rank - 1) % nranks, (rank + 1) % nranks
+
+
+def slab_group_flow(slabs: Sequence[GluonField], eps: float, nsteps: int, measure_every: int = 1,
+                    reunit_every: int = 0) -> np.ndarray:
+    """ymflow_flow over the slabs of one configuration held in this process
+    (in time order); rows (step, t, plaq, topc, energy, t2E) of the whole
+    configuration."""
+    rows = 1 + sum(1 for s in range(1, nsteps + 1)
+                   if (measure_every > 0 and s % measure_every == 0) or s == nsteps)
+    out = (N.Obs * rows)()
+    n = ctypes.c_int(0)
+    arr = (ctypes.c_void_p * len(slabs))(*[f.ctx for f in slabs])
+    N.check(N.load().ymflow_slab_group_flow(arr, len(slabs), float(eps), int(nsteps), int(measure_every),
+                                            int(reunit_every), out, rows, ctypes.byref(n)), slabs[0].ctx)
+    return np.array([out[i].as_tuple() for i in range(n.value)])
 
 
 def su3_exp(q: np.ndarray, device: int = 0) -> np.ndarray:

@@ -90,3 +90,21 @@ def test_big_endian_conf_round_trip(tmp_path):
     assert raw[:8] == U.reshape(-1)[:1].astype(">f8").tobytes()
     assert raw != (GOLDEN / "g4_expiah.bin").read_bytes()
     assert np.array_equal(read_conf(tmp_path / "be.bin", n, big_endian=True), U)
+
+
+def test_slab_partition_tiles_the_time_extent():
+    from latticeyangmills_b200 import slab_partition
+
+    for nt_global in (1, 7, 32, 33):
+        for nranks in range(1, min(nt_global, 9) + 1):
+            parts = [slab_partition(nt_global, nranks, r) for r in range(nranks)]
+            assert parts[0][0] == 0
+            assert sum(p[1] for p in parts) == nt_global
+            assert max(p[1] for p in parts) - min(p[1] for p in parts) <= 1
+            for r, (t0, nt, lo, hi) in enumerate(parts):
+                if r + 1 < nranks:
+                    assert parts[r + 1][0] == t0 + nt
+                assert parts[lo][0] + parts[lo][1] == t0 or (r == 0 and lo == nranks - 1)
+                assert parts[hi][2] == r
+    with pytest.raises(ValueError):
+        slab_partition(4, 5, 0)
