@@ -13,6 +13,12 @@ than the 126 MB L2 (no flush needed).
 Multi-GPU (torchrun, one rank per GPU): every rank flows its own configuration
 (replicas; the flow of independent configurations has no data-path exchange),
 timing is the max over ranks, `value` the sum of all ranks' link-updates.
+
+  python bench.py --decompose [--gpus N]   # ONE 32^4 configuration split along t
+
+--decompose times one configuration split into N time slabs, one per rank,
+with halos exchanged by NCCL after every stage (strong scaling).  At N = 1
+the single slab exchanges with itself, which prices the exchange on one GPU.
 """
 from __future__ import annotations
 
@@ -483,6 +489,72 @@ def our_arm(args, dist: Dist):
         print(json.dumps(line))
 
 
+def decomposed_run(args, dist: Dist):
+    """One configuration split along t over the ranks; NCCL halo exchange."""
+    import ctypes
+
+    import numpy as np
+
+    from latticeyangmills_b200 import GluonField, nccl_unique_id, slab_partition
+
+    prec = args.precision
+    V = DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]
+    t0, nt, lo, hi = slab_partition(DIMS[3], dist.world, dist.rank)
+    f = GluonField.slab(DIMS, t0, nt, prec, device=dist.local)
+    f.init_links("expiah", A, SEED)
+    if dist.world > 1:
+        box = [nccl_unique_id() if dist.rank == 0 else None]
+        dist.dist.broadcast_object_list(box, src=0)
+        nid = box[0]
+    else:
+        nid = nccl_unique_id()
+    f.connect(nid, dist.rank, dist.world, lo, hi)
+    f.time_steps(EPS, args.warmup)
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    time.sleep(0.5)
+    f.time_steps(EPS, max(args.warmup, 3))
+    dist.barrier()
+    elapsed_ms, _ = f.time_steps(EPS, args.steps)
+    dist.barrier()
+    _, kernel_ms = f.time_steps(EPS, args.steps, kernels=True)
+    clocks.stop()
+    t_max = dist.max(elapsed_ms / 1e3)
+    value = 4 * V * args.steps / t_max
+    peak, peak_kind = measured_peaks()
+    links_local = 4 * DIMS[0] * DIMS[1] * DIMS[2] * nt
+    bpl = bytes_per_link_update(prec) * links_local / 3.0
+    avg_launch_s = kernel_ms / 1e3 / (3 * args.steps)
+    # end to end: every rank uploads its slab from pinned host memory, flows, reads the rows
+    host = np.ascontiguousarray(f.download())
+    t0w = time.perf_counter()
+    f.upload(host)
+    rows = f.flow(EPS, args.steps, 0)
+    t_e2e = dist.max(time.perf_counter() - t0w)
+    f.close()
+    if dist.rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32" if prec != "fp64" else "f64",
+            "data": "synthetic (seeded U = e^{iaH}, a = 0.35, generated on the device)",
+            "config": {"workload": "one 32^4 configuration split along t, Luscher RK3, eps = 0.01",
+                       "lattice": list(DIMS), "precision": prec, "parallelism": "t-slabs x%d" % dist.world,
+                       "slices_per_rank": nt, "halo": "one time slice per side, NCCL send/recv after each stage",
+                       "kernel_share_of_step": kernel_ms / elapsed_ms,
+                       "l2": "inputs larger than L2 (links + generator > 126 MB per rank at N <= 2)"},
+            "roofline": {"bound": "hbm", "achieved": bpl / avg_launch_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": bpl / avg_launch_s / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "rk_stage_kernel on rank 0's slab", "avg_launch_ms": avg_launch_s * 1e3},
+            "e2e": {"value": 4 * V * args.steps / t_e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": host.nbytes * dist.world / args.steps,
+                    "d2h_bytes_per_step": 2 * 48 / args.steps,
+                    "what": "per rank: upload of its slab from host memory, a K-step collective flow, rows back",
+                    "t_end": float(rows[-1, 1])},
+            "gpu_launches": 3 * args.steps, "clocks": clocks.summary(), "cpu_baseline": None,
+        }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -497,6 +569,8 @@ def main():
     ap.add_argument("--workload", default="32", choices=["32", "16x32", "64"],
                     help="32: the headline 32^4 benchmark; 16x32 / 64: accuracy and throughput of the other "
                          "configurations against FP64")
+    ap.add_argument("--decompose", action="store_true",
+                    help="one 32^4 configuration split along t over the ranks (NCCL halo exchange)")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps of one precision (for ncu captures)")
     args = ap.parse_args()
@@ -514,7 +588,10 @@ def main():
         return
     dist = Dist(args.gpus)
     try:
-        our_arm(args, dist)
+        if args.decompose:
+            decomposed_run(args, dist)
+        else:
+            our_arm(args, dist)
     finally:
         dist.close()
 
