@@ -360,6 +360,14 @@ def our_arm(args, dist: Dist):
 
     f = GluonField(DIMS, prec, device=dev)
     f.init_links("expiah", A, seed)
+    if args.profile and args.profile_kernel == "obs":
+        # observables only (plaquette, clover energy and charge), for ncu captures
+        for _ in range(args.warmup + args.steps):
+            f.observables()
+        f.close()
+        if dist.rank == 0:
+            print(json.dumps({"profile": True, "kernel": "observables", "precision": prec, "lattice": list(DIMS)}))
+        return
     f.time_steps(EPS, args.warmup)  # untimed warm-up
 
     clocks = ClockSampler(dev)
@@ -569,6 +577,8 @@ def main():
     ap.add_argument("--workload", default="32", choices=["32", "16x32", "64"],
                     help="32: the headline 32^4 benchmark; 16x32 / 64: accuracy and throughput of the other "
                          "configurations against FP64")
+    ap.add_argument("--profile-kernel", default="stage", choices=["stage", "obs"],
+                    help="with --profile: the RK stage kernels or the observables kernel")
     ap.add_argument("--decompose", action="store_true",
                     help="one 32^4 configuration split along t over the ranks (NCCL halo exchange)")
     ap.add_argument("--profile", action="store_true",

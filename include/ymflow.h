@@ -178,7 +178,8 @@ YMFLOW_API int ymflow_time_steps(ymflow_ctx* ctx, double eps, int nsteps, float*
 
 /* Tuning knobs.  key YMFLOW_OPT_BLOCK: threads per block of the stage kernel
  * (128: four warps, one per direction, per 32 sites); YMFLOW_OPT_OBS_BLOCK:
- * threads per block of the observables kernel (32..256, multiple of 32);
+ * threads per block of the observables kernel (192: six warps, one per
+ * plane, per 32 sites; read-only in effect, other values are rejected);
  * YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a captured CUDA graph
  * (default), 0 = plain launches. */
 #define YMFLOW_OPT_BLOCK 1

@@ -35,7 +35,6 @@ struct ymflow_ctx {
     std::vector<cudaEvent_t> events;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int block = 128;
-    int obs_block = 128;
     bool use_graph = true;
     bool loaded = false;
     int64_t step = 0;

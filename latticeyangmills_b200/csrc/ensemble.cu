@@ -140,7 +140,6 @@ struct ymflow_ens {
     int graph_cfg[2][2] = {{0, 0}, {0, 0}};
     int block = 128;
     int grid = 0;  // persistent CTAs (0: one per work item)
-    int obs_block = 128;
     bool use_graph = true;
     bool tuned = false;
     std::vector<char> loaded;
@@ -271,8 +270,8 @@ int enqueue_ens_measure(ymflow_ens* e, int row) {
     for (int c = 0; c < e->nconf; c++) {
         const EnsConf& C = e->confs[c];
         const void* u = (const char*)e->u[e->cur] + C.uoff;
-        YE_CK(e, launch_observables(e->prec, u, C.g, e->partials, e->obs_block, e->stream), "observables launch");
-        YE_CK(e, launch_obs_finalize(e->partials, obs_blocks(C.g, e->obs_block), C.g,
+        YE_CK(e, launch_observables(e->prec, u, C.g, e->partials, e->stream), "observables launch");
+        YE_CK(e, launch_obs_finalize(e->partials, obs_blocks(C.g), C.g,
                                      e->meas + 4 * (size_t(row) * e->nconf + c), e->stream),
               "observables fold");
     }
@@ -370,8 +369,10 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->confs_dev, sizeof(EnsConf) * nconf, "work list");
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->deviation, sizeof(unsigned long long), "drift flag");
     if (r == YMFLOW_OK) {
-        // most observable blocks of any configuration: the largest one at the smallest block (32)
-        e->partial_cap = std::max(int((e->max_v + 31) / 32), 1);
+        // most observable blocks of any configuration (the kernel's grid is capped)
+        int cap = 1;
+        for (const EnsConf& C : e->confs) cap = std::max(cap, obs_blocks(C.g));
+        e->partial_cap = cap;
         r = ens_alloc(e, (void**)&e->partials, size_t(e->partial_cap) * 3 * sizeof(double), "partials");
     }
     if (r == YMFLOW_OK && (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess))

@@ -32,12 +32,12 @@ cudaError_t launch_force(int prec, int mu, const void* u, const Geo& g, double* 
 // e^{iQ} for n Hermitian traceless matrices (18 doubles each).
 cudaError_t launch_exp(const double* q, double* r, int64_t n, cudaStream_t st);
 
-// Observables: per-block FP64 partial sums (plaq, energy, topc) into partials[3*nblocks],
-// then one block folds them in a fixed order into out[3] = (plaq, topc, energy) with the
-// reference's normalisations, out[3] = 1.0 when any value is not finite.
-int obs_blocks(const Geo& g, int block);
-cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* partials, int block,
-                               cudaStream_t st);
+// Observables of the sites [g.site0, g.site1): per-block FP64 partial sums (plaq, energy,
+// topc) into partials[3 * obs_blocks(g)], then one block folds them in a fixed order into
+// out[3] = (plaq, topc, energy) with the reference's normalisations, out[3] = 1.0 when any
+// value is not finite.
+int obs_blocks(const Geo& g);
+cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* partials, cudaStream_t st);
 cudaError_t launch_obs_finalize(const double* partials, int nblocks, const Geo& g, double* out, cudaStream_t st);
 
 // .bin layout (site-major, mu, 18 doubles) <-> device layout

@@ -114,7 +114,7 @@ extern "C" int ymflow_observables_noalloc(const double* links_aos_device, const 
     const Geo g = make_geo(dims);
     const int nb = int((g.V + kNoAllocBlock - 1) / kNoAllocBlock);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    observables_kernel<<<nb, kNoAllocBlock, 0, st>>>(AosField{links_aos_device, g.V}, g, partials);
+    observables_site_kernel<<<nb, kNoAllocBlock, 0, st>>>(AosField{links_aos_device, g.V}, g, partials);
     if (cudaGetLastError() != cudaSuccess) return YMFLOW_ERR_CUDA;
     if (launch_obs_finalize(partials, nb, g, out_device, st) != cudaSuccess) return YMFLOW_ERR_CUDA;
     return YMFLOW_OK;

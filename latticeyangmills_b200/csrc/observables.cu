@@ -1,5 +1,5 @@
 // K2: plaquette, clover energy and clover topological charge
-// (src/Observables/superobs.cpp:31-128), one thread per site.
+// (src/Observables/superobs.cpp:31-128), one thread per (site, plane).
 //
 // Per plane (mu < nu) the four clover leaves, all oriented the same way,
 //   Q1 = U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
@@ -43,21 +43,24 @@ __global__ void __launch_bounds__(1024) obs_finalize_kernel(const double* partia
     }
 }
 
-int obs_blocks(const Geo& g, int block) { return int((g.site1 - g.site0 + block - 1) / block); }
+int obs_blocks(const Geo& g) {
+    const int groups = (g.site1 - g.site0 + kObsSites - 1) / kObsSites;
+    return groups < kObsMaxBlocks ? groups : kObsMaxBlocks;
+}
 
-cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* partials, int block, cudaStream_t st) {
-    const unsigned nb = unsigned(obs_blocks(g, block));
+cudaError_t launch_observables(int prec, const void* u, const Geo& g, double* partials, cudaStream_t st) {
+    const unsigned nb = unsigned(obs_blocks(g));
+    if (nb == 0) return cudaErrorInvalidValue;
     switch (prec) {
         case kFP64:
-            observables_kernel<<<nb, block, 0, st>>>(FieldD18{const_cast<void*>(u), g.V}, g, partials);
+            observables_kernel<<<nb, kObsThreads, 0, st>>>(FieldD18{const_cast<void*>(u), g.V}, g, partials);
             break;
         case kFP32_18:
-            observables_kernel<<<nb, block, 0, st>>>(FieldF18{const_cast<void*>(u), g.V}, g, partials);
+            observables_kernel<<<nb, kObsThreads, 0, st>>>(FieldF18{const_cast<void*>(u), g.V}, g, partials);
             break;
         case kFP32_12:
-            observables_kernel<<<nb, block, 0, st>>>(FieldF12{const_cast<void*>(u), g.V}, g, partials);
+            observables_kernel<<<nb, kObsThreads, 0, st>>>(FieldF12{const_cast<void*>(u), g.V}, g, partials);
             break;
-
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -60,7 +60,7 @@ int ensure_staging(ymflow_ctx* c, size_t bytes = 0) {
 }
 
 int ensure_partials(ymflow_ctx* c) {
-    const int nb = obs_blocks(c->geo, c->obs_block);
+    const int nb = obs_blocks(c->geo);
     if (nb <= c->partial_cap) return YMFLOW_OK;
     if (c->partials) {
         cudaFree(c->partials);
@@ -177,9 +177,9 @@ namespace ym {
 int enqueue_measure(ymflow_ctx* c, int row) {
     int r = ensure_partials(c);
     if (r != YMFLOW_OK) return r;
-    YM_CK(c, launch_observables(c->prec, c->u[c->cur], c->geo, c->partials, c->obs_block, c->stream),
+    YM_CK(c, launch_observables(c->prec, c->u[c->cur], c->geo, c->partials, c->stream),
           "observables launch");
-    YM_CK(c, launch_obs_finalize(c->partials, obs_blocks(c->geo, c->obs_block), c->geo, c->meas + 4 * row, c->stream),
+    YM_CK(c, launch_obs_finalize(c->partials, obs_blocks(c->geo), c->geo, c->meas + 4 * row, c->stream),
           "observables fold");
     if (c->slab && c->comm) return slab_reduce_row(c, c->meas + 4 * row);
     return YMFLOW_OK;
@@ -634,9 +634,8 @@ int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
             if (value != 128) return fail(c, YMFLOW_ERR_ARG, "stage block must be 128 (compiled launch bounds)");
             c->block = int(value);
             return YMFLOW_OK;
-        case YMFLOW_OPT_OBS_BLOCK:
-            if (value < 32 || value > 256 || value % 32) return fail(c, YMFLOW_ERR_ARG, "block must be 32..256, /32");
-            c->obs_block = int(value);
+        case YMFLOW_OPT_OBS_BLOCK:  // fixed: six warps (one per plane) per 32 sites
+            if (value != 192) return fail(c, YMFLOW_ERR_ARG, "observables block is 192 (six warps per 32 sites)");
             return YMFLOW_OK;
         case YMFLOW_OPT_GRAPH:
             c->use_graph = value != 0;
@@ -649,7 +648,7 @@ int ymflow_get_option(const ymflow_ctx* c, int key, int64_t* value) {
     if (!c || !value) return YMFLOW_ERR_ARG;
     switch (key) {
         case YMFLOW_OPT_BLOCK: *value = c->block; return YMFLOW_OK;
-        case YMFLOW_OPT_OBS_BLOCK: *value = c->obs_block; return YMFLOW_OK;
+        case YMFLOW_OPT_OBS_BLOCK: *value = 192; return YMFLOW_OK;
         case YMFLOW_OPT_GRAPH: *value = c->use_graph ? 1 : 0; return YMFLOW_OK;
         default: return YMFLOW_ERR_ARG;
     }

@@ -111,11 +111,12 @@ def test_graph_and_block_size_do_not_change_results():
     case = load_case("g3456_expiah")
     U = case_field(case)
     outs = []
-    for graph, block, obs_block in [(1, 128, 128), (0, 128, 64), (1, 128, 256), (0, 128, 32)]:
+    for graph, block, obs_block in [(1, 128, 192), (0, 128, 192)]:
         with GluonField(tuple(case["dims"]), "fp64") as f:
             f.set_option(N.OPT_GRAPH, graph)
             f.set_option(N.OPT_BLOCK, block)
             f.set_option(N.OPT_OBS_BLOCK, obs_block)
+            assert f.get_option(N.OPT_OBS_BLOCK) == 192
             f.upload(U)
             rows = f.flow(case["eps"], 4, 0)
             outs.append((f.download(), rows))
