@@ -41,6 +41,24 @@ def test_flow_app_output_matches_reference_app(tmp_path):
     assert (tmp_path / "out" / "flow" / "conf0000.full.dat").exists()
 
 
+REF_GPU_APP = ROOT / "oracle" / "_ref" / "lattice_qcd_ymflow"
+
+
+@pytest.mark.skipif(not REF_GPU_APP.exists(), reason="oracle/_ref/lattice_qcd_ymflow not built (no reference tree)")
+def test_reference_application_with_gpu_wilsonflow(tmp_path):
+    """The reference's own LatticeQCD program (its main, JSON layer and I/O)
+    with its WilsonFlow replaced by the libymflow adapter
+    (latticeyangmills_b200/adapter/wilsonflow_ymflow.cpp): the same terminal
+    lines and files as the unmodified reference application."""
+    run = prepare(tmp_path)
+    res = subprocess.run([str(REF_GPU_APP), str(run)], capture_output=True, text=True, check=True)
+    got = [l for l in res.stdout.splitlines(keepends=True) if not l.startswith("Total time taken")]
+    exp = GOLDEN / "app_flow" / "expected"
+    assert "".join(got) == (exp / "stdout.txt").read_text()
+    for f in ["observables.dat", "flow/conf0000.dat", "flow/conf0001.dat"]:
+        assert (tmp_path / "out" / f).read_bytes() == (exp / f).read_bytes(), f
+
+
 def test_flow_app_big_endian_streamed_input(tmp_path):
     """Byte-reversed ("Chroma") inputs read in ragged chunks give the same
     files as the native-endian run."""

@@ -108,3 +108,20 @@ def test_slab_partition_tiles_the_time_extent():
                 assert parts[hi][2] == r
     with pytest.raises(ValueError):
         slab_partition(4, 5, 0)
+
+
+REF_GPU_APP = ROOT / "oracle" / "_ref" / "lattice_qcd_ymflow"
+
+
+@pytest.mark.skipif(not REF_GPU_APP.exists(), reason="oracle/_ref/lattice_qcd_ymflow not built (no reference tree)")
+def test_reference_registry_reaches_the_gpu_wilsonflow(tmp_path):
+    """The reference's JSON layer builds its FLOW app from the adapter's
+    WilsonFlow: without a B200 the adapter's device set-up is what stops it."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: tests/test_gpu_app.py runs the application")
+    run = _app_input(tmp_path, {})
+    res = subprocess.run([str(REF_GPU_APP), str(run)], capture_output=True, text=True)
+    assert res.returncode == 1
+    assert "ymflow create" in res.stderr
