@@ -305,26 +305,41 @@ def workload_run(args, dev: int):
     from the same seeded field, with each observable's error against FP64:
       16x32: 16^3 x 32, a = 0.35, eps 0.01 to t = 2, observables every 10 steps
       64:    64^4, a = 0.35 plus 5 % Haar-random links, eps 0.02 to t = 6,
-             observables every 5 steps (about 24 GB in FP64)."""
+             observables every 5 steps (about 24 GB in FP64)
+      8:     8^4 Metropolis field (beta 6, 200 sweeps of 30 hits from cold, made by the
+             device generator in FP64), eps 0.01, 100 steps, observables every step."""
     import time
 
     import numpy as np
 
     from latticeyangmills_b200 import GluonField
 
+    field = None
     if args.workload == "16x32":
         dims, a, haar, eps, nsteps, every = (16, 16, 16, 32), A, 0.0, 0.01, 200, 10
+    elif args.workload == "8":
+        dims, a, haar, eps, nsteps, every = (8, 8, 8, 8), 0.0, 0.0, 0.01, 100, 1
+        with GluonField(dims, "fp64", device=dev) as g:
+            acceptance = g.generate_metropolis(6.0, 0.24, 200, 30, SEED, "cold")
+            field = g.download()
     else:
         dims, a, haar, eps, nsteps, every = (64, 64, 64, 64), A, 0.05, 0.02, 300, 5
     links = 4 * dims[0] * dims[1] * dims[2] * dims[3]
+
+    def load(f):
+        if field is None:
+            f.init_links("expiah", a, SEED, 0, haar)
+        else:
+            f.upload(field)
+
     res = {}
     for p in ["fp64", "fp32_18", "fp32_12"]:
         f = GluonField(dims, p, device=dev)
-        f.init_links("expiah", a, SEED, 0, haar)
+        load(f)
         t0 = time.perf_counter()
         rows = f.flow(eps, nsteps, every, reunit_every=10 if p != "fp64" else 0)
         wall = time.perf_counter() - t0
-        f.init_links("expiah", a, SEED, 0, haar)
+        load(f)
         f.time_steps(eps, 3)
         ms, _ = f.time_steps(eps, 20)
         f.close()
@@ -333,6 +348,9 @@ def workload_run(args, dev: int):
     out = {"workload": args.workload, "lattice": list(dims), "eps": eps, "steps": nsteps, "measure_every": every,
            "haar_fraction": haar, "t_final": float(r64[-1, 1]), "t2E_fp64_final": float(r64[-1, 5]),
            "Q_fp64_final": float(r64[-1, 3])}
+    if field is not None:
+        out.update({"field": "Metropolis beta 6, 200 sweeps x 30 hits, su3eps 0.24, from cold",
+                    "metropolis_acceptance": acceptance, "plaq_t0": float(r64[0, 2])})
     for p in ["fp64", "fp32_18", "fp32_12"]:
         rows, lups, wall = res[p]
         d = {"link_updates_per_s": lups, "flow_wall_s_with_measurements": wall}
@@ -574,9 +592,9 @@ def main():
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--lattice", type=int, default=32, help="L of the L^4 lattice (profiling of smaller cases)")
-    ap.add_argument("--workload", default="32", choices=["32", "16x32", "64"],
-                    help="32: the headline 32^4 benchmark; 16x32 / 64: accuracy and throughput of the other "
-                         "configurations against FP64")
+    ap.add_argument("--workload", default="32", choices=["32", "16x32", "64", "8"],
+                    help="32: the headline 32^4 benchmark; 8 / 16x32 / 64: accuracy and throughput of the "
+                         "other configurations against FP64")
     ap.add_argument("--profile-kernel", default="stage", choices=["stage", "obs"],
                     help="with --profile: the RK stage kernels or the observables kernel")
     ap.add_argument("--decompose", action="store_true",
