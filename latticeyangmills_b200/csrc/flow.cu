@@ -36,6 +36,37 @@ __global__ void __launch_bounds__(128, StageMinBlocks<F>::value)
     rk_link_update<F, STAGE>(in, out, zf, g, eps, s, mu);
 }
 
+// The same stage for a slab whose boundary links also go straight into its
+// neighbours' halos: the halo exchange fused into the stage.
+template <class F, int STAGE>
+__global__ void __launch_bounds__(128, StageMinBlocks<F>::value)
+    rk_stage_halo_kernel(F in, F out, ForceField<typename F::Real> zf, Geo g, typename F::Real eps,
+                         HaloTargets<F> h) {
+    int s;
+    int mu;
+    link_of_thread(g, s, mu);
+    if (s >= g.site1) return;
+    rk_link_update_to<F, STAGE, true>(in, out, zf, g, eps, s, mu, h);
+}
+
+template <class F>
+static cudaError_t launch_halo_typed(int stage, const void* uin, void* uout, void* z, const Geo& g, double eps,
+                                     void* lower_out, int lower_v, int lower_t, void* upper_out, int upper_v,
+                                     cudaStream_t st) {
+    using R = typename F::Real;
+    F in{const_cast<void*>(uin), g.V}, out{uout, g.V};
+    ForceField<R> zf{z, g.V};
+    HaloTargets<F> h{F{lower_out, lower_v}, F{upper_out, upper_v}, g.site0, (g.site1 - g.site0) / g.site0, lower_t};
+    dim3 grid(unsigned((g.site1 - g.site0 + 31) / 32));
+    const R e = R(stage == 0 ? eps * 0.25 : eps);
+    switch (stage) {
+        case 0: rk_stage_halo_kernel<F, 0><<<grid, 128, 0, st>>>(in, out, zf, g, e, h); break;
+        case 1: rk_stage_halo_kernel<F, 1><<<grid, 128, 0, st>>>(in, out, zf, g, e, h); break;
+        default: rk_stage_halo_kernel<F, 2><<<grid, 128, 0, st>>>(in, out, zf, g, e, h); break;
+    }
+    return cudaGetLastError();
+}
+
 template <class F>
 static cudaError_t launch_typed(int stage, const void* uin, void* uout, void* z, const Geo& g, double eps, int block,
                                 cudaStream_t st) {
@@ -116,6 +147,24 @@ cudaError_t launch_exp(const double* q, double* r, int64_t n, cudaStream_t st) {
     const int b = 128;
     exp_kernel<<<unsigned((n + b - 1) / b), b, 0, st>>>(q, r, n);
     return cudaGetLastError();
+}
+
+cudaError_t launch_rk_stage_halo(int prec, int stage, const void* uin, void* uout, void* z, const Geo& g, double eps,
+                                 void* lower_out, int lower_v, int lower_t, void* upper_out, int upper_v,
+                                 cudaStream_t st) {
+    if (g.site0 <= 0 || g.site0 % 32 || (g.site1 - g.site0) % g.site0) return cudaErrorInvalidValue;
+    switch (prec) {
+        case kFP64:
+            return launch_halo_typed<FieldD18>(stage, uin, uout, z, g, eps, lower_out, lower_v, lower_t, upper_out,
+                                               upper_v, st);
+        case kFP32_18:
+            return launch_halo_typed<FieldF18>(stage, uin, uout, z, g, eps, lower_out, lower_v, lower_t, upper_out,
+                                               upper_v, st);
+        case kFP32_12:
+            return launch_halo_typed<FieldF12>(stage, uin, uout, z, g, eps, lower_out, lower_v, lower_t, upper_out,
+                                               upper_v, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_rk_stage(int prec, int stage, const void* uin, void* uout, void* z, const Geo& g, double eps,

@@ -92,9 +92,24 @@ __device__ __forceinline__ Herm8<typename F::Real> link_force(const F& in, const
 
 // One link through one RK3 stage: generator, RK combination with the stored
 // generator, e^{i eps_s Z} and the update of the link from `in` into `out`.
-template <class F, int STAGE>
-__device__ __forceinline__ void rk_link_update(const F& in, const F& out, const ForceField<typename F::Real>& zf,
-                                               const Geo& g, typename F::Real eps, int s, int mu) {
+// Where a slab's new boundary links also go, for a time slab of a decomposed
+// configuration: the neighbouring slabs' output buffers of the same stage
+// (peer pointers when they sit on other GPUs).  Local slice 1 is the lower
+// slab's upper halo (its slice lower_t = its nt + 1), local slice nt the upper
+// slab's lower halo (its slice 0).  A slab's own kernel never writes its
+// halo slices, so these stores race with nothing.
+template <class F>
+struct HaloTargets {
+    F lower, upper;
+    int slice_sites;  // sites per time slice (a multiple of 32)
+    int nt;           // this slab's interior slices
+    int lower_t;
+};
+
+template <class F, int STAGE, bool HALO>
+__device__ __forceinline__ void rk_link_update_to(const F& in, const F& out, const ForceField<typename F::Real>& zf,
+                                                  const Geo& g, typename F::Real eps, int s, int mu,
+                                                  const HaloTargets<F>& h) {
     using R = typename F::Real;
     int c[4];
     g.coords(s, c);
@@ -115,6 +130,16 @@ __device__ __forceinline__ void rk_link_update(const F& in, const F& out, const 
     exp_iq_rows2(q, e);
     mmul_rows2<false, false>(e, u, un);  // e^{iQ} U is in SU(3): two rows suffice
     out.store_rows2(mu, s, un);
+    if constexpr (HALO) {
+        if (c[3] == 1) h.lower.store_rows2(mu, h.lower_t * h.slice_sites + (s - h.slice_sites), un);
+        if (c[3] == h.nt) h.upper.store_rows2(mu, s - h.nt * h.slice_sites, un);
+    }
+}
+
+template <class F, int STAGE>
+__device__ __forceinline__ void rk_link_update(const F& in, const F& out, const ForceField<typename F::Real>& zf,
+                                               const Geo& g, typename F::Real eps, int s, int mu) {
+    rk_link_update_to<F, STAGE, false>(in, out, zf, g, eps, s, mu, HaloTargets<F>{});
 }
 
 }  // namespace ym

@@ -26,6 +26,14 @@ inline bool volume_addressable(int prec, int64_t V) { return link_field_bytes(pr
 cudaError_t launch_rk_stage(int prec, int stage, const void* uin, void* uout, void* z, const Geo& g, double eps,
                             int block, cudaStream_t st);
 
+// The same stage for a time slab (g.site0 = sites per slice, interior slices
+// [1, nt]): each new link of local slice 1 is also stored into the lower slab's
+// buffer lower_out (lower_v sites) at its slice lower_t, and each of slice nt
+// into upper_out's slice 0: the halo exchange inside the stage kernel.
+cudaError_t launch_rk_stage_halo(int prec, int stage, const void* uin, void* uout, void* z, const Geo& g, double eps,
+                                 void* lower_out, int lower_v, int lower_t, void* upper_out, int upper_v,
+                                 cudaStream_t st);
+
 // D_mu (18 doubles per site, site order) for one direction: the reference's
 // PureGauge::computeDerivative(mu).
 cudaError_t launch_force(int prec, int mu, const void* u, const Geo& g, double* out, cudaStream_t st);

@@ -14,10 +14,15 @@
 //    grouped ncclSend/ncclRecv on the context's stream and sum each
 //    measurement row with ncclAllReduce.  NCCL is loaded at run time
 //    (libnccl.so.2), so the library needs it only when this is used.
-//  * Peer copies inside one process: ymflow_slab_group_flow flows the slab
-//    contexts of one configuration (on one or several GPUs) stage by stage,
-//    each halo a stream-ordered cudaMemcpyPeerAsync after an event wait on the
-//    neighbour's stage; no kernel waits on another.
+//  * Inside one process: ymflow_slab_group_flow flows the slab contexts of one
+//    configuration (on one or several GPUs) stage by stage.  Each slab's stage
+//    kernel also stores its new boundary links straight into its neighbours'
+//    halo slices (peer stores over NVLink when they sit on other GPUs): the
+//    exchange is part of the stage.  Before the next stage every slab's stream
+//    waits for both neighbours' stage events; no kernel waits on another.
+//    Where two GPUs cannot reach each other's memory (or with
+//    YMFLOW_SLAB_COPY_EXCHANGE set) the halos are cudaMemcpyPeerAsync copies
+//    after the stage instead.
 //
 // In the warp-group layout a time slice of one direction is one contiguous run
 // of the link buffer (the slab's spatial volume is a multiple of 32 sites), so
@@ -26,6 +31,7 @@
 #include <nccl.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -178,6 +184,39 @@ int group_exchange(ymflow_ctx* const* cs, int n, const int* buf, std::vector<cud
     return YMFLOW_OK;
 }
 
+// After every slab's fused stage: each slab's next work waits for both
+// neighbours' stages, which wrote its halos.
+int group_order(ymflow_ctx* const* cs, int n, std::vector<cudaEvent_t>& ev) {
+    for (int i = 0; i < n; i++) {
+        DeviceGuard g(cs[i]->device);
+        YM_CK(cs[i], cudaEventRecord(ev[i], cs[i]->stream), "event record");
+    }
+    for (int i = 0; i < n; i++) {
+        DeviceGuard g(cs[i]->device);
+        YM_CK(cs[i], cudaStreamWaitEvent(cs[i]->stream, ev[(i + n - 1) % n], 0), "wait lower slab");
+        YM_CK(cs[i], cudaStreamWaitEvent(cs[i]->stream, ev[(i + 1) % n], 0), "wait upper slab");
+    }
+    return YMFLOW_OK;
+}
+
+// Whether kernels on `from` can store into `to`'s memory (enabling peer access once).
+bool peer_reachable(int from, int to) {
+    if (from == to) return true;
+    int ok = 0;
+    if (cudaDeviceCanAccessPeer(&ok, from, to) != cudaSuccess || !ok) {
+        cudaGetLastError();
+        return false;
+    }
+    DeviceGuard g(from);
+    const cudaError_t e = cudaDeviceEnablePeerAccess(to, 0);
+    if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaGetLastError();
+    return true;
+}
+
 }  // namespace
 }  // namespace ym
 
@@ -252,6 +291,11 @@ int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nstep
         YM_CK(ctxs[i], cudaEventCreateWithFlags(&evs.ev[i], cudaEventDisableTiming), "event create");
     }
     const bool reunit = c0->prec != YMFLOW_FP64 && reunit_every > 0;
+    // the fused exchange needs every slab's GPU to reach its neighbours' memory
+    bool fused = std::getenv("YMFLOW_SLAB_COPY_EXCHANGE") == nullptr;
+    for (int i = 0; i < n && fused; i++)
+        for (int j : {(i + n - 1) % n, (i + 1) % n})
+            if (fused && !peer_reachable(ctxs[i]->device, ctxs[j]->device)) fused = false;
     std::vector<int> buf(static_cast<size_t>(n));
     auto exchange_current = [&]() {
         for (int i = 0; i < n; i++) buf[i] = ctxs[i]->cur;
@@ -281,15 +325,31 @@ int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nstep
     int row = 1;
     for (int s = 1; s <= nsteps; s++) {
         for (int stage = 0; stage < 3; stage++) {
-            for (int i = 0; i < n; i++) {
-                ymflow_ctx* c = ctxs[i];
-                DeviceGuard g(c->device);
-                YM_CK(c, launch_rk_stage(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z, c->geo, eps, c->block,
-                                         c->stream),
-                      "stage launch");
-                c->cur = 1 - c->cur;
+            if (fused) {
+                // each slab's stage stores its boundary links into its neighbours' halos itself
+                for (int i = 0; i < n; i++) {
+                    ymflow_ctx* c = ctxs[i];
+                    ymflow_ctx* lo = ctxs[(i + n - 1) % n];
+                    ymflow_ctx* hi = ctxs[(i + 1) % n];
+                    DeviceGuard g(c->device);
+                    YM_CK(c, launch_rk_stage_halo(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z, c->geo, eps,
+                                                  lo->u[1 - lo->cur], lo->geo.V, lo->nt + 1, hi->u[1 - hi->cur],
+                                                  hi->geo.V, c->stream),
+                          "stage launch");
+                }
+                for (int i = 0; i < n; i++) ctxs[i]->cur = 1 - ctxs[i]->cur;
+                if ((r = group_order(ctxs, n, evs.ev)) != YMFLOW_OK) return r;
+            } else {
+                for (int i = 0; i < n; i++) {
+                    ymflow_ctx* c = ctxs[i];
+                    DeviceGuard g(c->device);
+                    YM_CK(c, launch_rk_stage(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z, c->geo, eps,
+                                             c->block, c->stream),
+                          "stage launch");
+                    c->cur = 1 - c->cur;
+                }
+                if ((r = exchange_current()) != YMFLOW_OK) return r;
             }
-            if ((r = exchange_current()) != YMFLOW_OK) return r;
         }
         for (int i = 0; i < n; i++) {
             ymflow_ctx* c = ctxs[i];

@@ -20,6 +20,13 @@ def whole(precision, n=N8, seed=11, steps=6, every=2):
         return U0, rows, f.download()
 
 
+def close_rows(got, want, precision):
+    """plaquette, energy and t^2 E relative; the charge absolute (it crosses zero)."""
+    rtol, qtol = (1e-12, 1e-12) if precision == "fp64" else (1e-6, 1e-6)
+    np.testing.assert_allclose(got[:, [2, 4, 5]], want[:, [2, 4, 5]], rtol=rtol, atol=1e-15)
+    assert np.abs(got[:, 3] - want[:, 3]).max() < qtol
+
+
 def split(n, parts):
     t0 = 0
     for nt in parts:
@@ -44,10 +51,42 @@ def test_group_flow_matches_whole_lattice(precision, parts):
     finally:
         for s in slabs:
             s.close()
-    assert np.array_equal(after, U1)
+    # The slabs' stage kernel stores its boundary links into its neighbours'
+    # halos as well; it is a separate kernel, whose FP32 multiply-adds the
+    # compiler may fuse differently: FP64 is bit-identical, FP32 equal to its
+    # rounding.
+    diff = np.abs(after - U1).max()
+    print(precision, parts, "max |dU|", diff, "max |d obs|", np.abs(got[:, 2:] - rows[:, 2:]).max())
+    assert diff == 0.0 if precision == "fp64" else diff < 1e-5
     assert got.shape == rows.shape
     assert np.array_equal(got[:, :2], rows[:, :2])
-    np.testing.assert_allclose(got[:, 2:], rows[:, 2:], rtol=1e-12, atol=1e-15)
+    close_rows(got, rows, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_18"])
+def test_copy_exchange_matches_fused_exchange(precision, monkeypatch):
+    """The halo exchange as copies after each stage (the fallback for GPUs
+    that cannot reach each other's memory) gives the same links as the
+    exchange fused into the stage kernel."""
+    from latticeyangmills_b200 import GluonField, slab_group_flow
+
+    out = {}
+    for mode in ("fused", "copy"):
+        if mode == "copy":
+            monkeypatch.setenv("YMFLOW_SLAB_COPY_EXCHANGE", "1")
+        slabs = [GluonField.slab(N8, t0, nt, precision) for t0, nt in split(N8, (4, 3, 3))]
+        try:
+            for sl in slabs:
+                sl.init_links("expiah", 0.4, 11)
+            rows = slab_group_flow(slabs, 0.02, 6, 3)
+            out[mode] = (rows, np.concatenate([sl.download() for sl in slabs]))
+        finally:
+            for sl in slabs:
+                sl.close()
+    diff = np.abs(out["fused"][1] - out["copy"][1]).max()
+    print(precision, "fused vs copy max |dU|", diff)
+    assert diff == 0.0 if precision == "fp64" else diff < 1e-5
+    close_rows(out["fused"][0], out["copy"][0], precision)
 
 
 def test_uploaded_slabs_match_whole_lattice():
@@ -82,7 +121,7 @@ def test_nccl_single_rank_slab_matches_whole_lattice(precision):
         got = s.flow(0.02, 6, 2, reunit_every=3 if precision != "fp64" else 0)
         after = s.download()
     assert np.array_equal(after, U1)
-    np.testing.assert_allclose(got[:, 2:], rows[:, 2:], rtol=1e-12, atol=1e-15)
+    close_rows(got, rows, precision)
     assert abs(o.plaq - rows[0, 2]) < 1e-14
 
 
