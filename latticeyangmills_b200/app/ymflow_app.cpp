@@ -28,9 +28,13 @@
 // and the terminal lines of outputterm.cpp.  Added: OutputDir/flow/confNNNN.full.dat
 // with every number at full precision ("%.17g") and t^2<E>.
 //
-// The whole lattice lives on one GPU, so SubLatticeSize is validated but not
-// used for a decomposition (the reference on one rank requires it to equal
-// LatticeSize, parallel.cpp:57-70).
+// SubLatticeSize: the reference splits the lattice into sub-lattices, one per
+// MPI rank (parallel.cpp:57-100).  When it splits only the time extent (x, y,
+// z equal to LatticeSize's, t dividing it), this driver flows each
+// configuration as that many time slabs, one per GPU (round-robin over the
+// B200s present from "Device"), with the halo exchange inside the stage kernel
+// (ymflow_slab_group_flow).  Any other SubLatticeSize is validated and the
+// lattice flows whole on one GPU.
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -77,6 +81,7 @@ void read_extents(const jl::Value& root, const char* key, int out[4]) {
     for (int i = 0; i < 4; i++) {
         if (v[names[i]].kind != jl::Value::Number) die(std::string(key) + " extents must be numbers");
         out[i] = int(v[names[i]].num);
+        if (out[i] < 1) die(std::string(key) + " extents must be >= 1");
     }
 }
 
@@ -182,8 +187,17 @@ int main(int argc, char** argv) {
 
     std::printf("Total Lattice Size: %2i %2i %2i %2i\n", in.size[0], in.size[1], in.size[2], in.size[3]);
     std::printf("Sublattice Size:    %2i %2i %2i %2i\n\n", in.sub[0], in.sub[1], in.sub[2], in.sub[3]);
-    std::printf("Number of Processors: \t\t%i\n", 1);
-    std::printf("Number of Active Processors: \t%i\n\n", 1);
+    // time slabs when SubLatticeSize splits only t
+    int nslabs = 1;
+    if (in.sub[0] == in.size[0] && in.sub[1] == in.size[1] && in.sub[2] == in.size[2] && in.sub[3] < in.size[3] &&
+        in.size[3] % in.sub[3] == 0) {
+        if ((int64_t(in.size[0]) * in.size[1] * in.size[2]) % 32 == 0)
+            nslabs = in.size[3] / in.sub[3];
+        else
+            std::fprintf(stderr, "ymflow: time slabs need x y z divisible by 32; flowing the lattice whole\n");
+    }
+    std::printf("Number of Processors: \t\t%i\n", nslabs);
+    std::printf("Number of Active Processors: \t%i\n\n", nslabs);
 
     mkdir(in.output_dir.c_str(), 0755);
     mkdir((in.output_dir + "/flow").c_str(), 0755);
@@ -195,8 +209,23 @@ int main(int argc, char** argv) {
     }
 
     int st = 0;
-    ymflow_ctx* ctx = ymflow_create(in.size, in.precision, in.device, &st);
-    if (!ctx) die(std::string("ymflow_create: ") + ymflow_last_error(nullptr));
+    std::vector<ymflow_ctx*> slabs;  // one context per slab (one slab: the whole lattice)
+    if (nslabs == 1) {
+        ymflow_ctx* ctx = ymflow_create(in.size, in.precision, in.device, &st);
+        if (!ctx) die(std::string("ymflow_create: ") + ymflow_last_error(nullptr));
+        slabs.push_back(ctx);
+    } else {
+        int ndev = 0;
+        ymflow_device_count(&ndev);
+        for (int i = 0; i < nslabs; i++) {
+            const int dev = ndev > 0 ? (in.device + i) % ndev : in.device;
+            ymflow_ctx* c = ymflow_create_slab(in.size, i * in.sub[3], in.sub[3], in.precision, dev, &st);
+            if (!c) die(std::string("ymflow_create_slab: ") + ymflow_last_error(nullptr));
+            slabs.push_back(c);
+        }
+    }
+    ymflow_ctx* ctx = slabs[0];
+    const int64_t slab_sites = int64_t(in.size[0]) * in.size[1] * in.size[2] * (nslabs > 1 ? in.sub[3] : in.size[3]);
 
     const int64_t V = int64_t(in.size[0]) * in.size[1] * in.size[2] * in.size[3];
     const int64_t chunk = std::min<int64_t>(in.chunk_sites, V);
@@ -219,12 +248,26 @@ int main(int argc, char** argv) {
                 std::fclose(f);
                 die(path + ": shorter than the LatticeSize configuration");
             }
-            check(ymflow_upload_sites(ctx, buf, first, n, in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0), ctx, "upload");
+            // the chunk's sites, slab by slab (each slab holds a contiguous range of the file)
+            for (int64_t done = 0; done < n;) {
+                const int64_t site = first + done;
+                const int k = int(site / slab_sites);
+                const int64_t m = std::min(n - done, (k + 1) * slab_sites - site);
+                check(ymflow_upload_sites(slabs[k], buf + done * 72, site - k * slab_sites, m,
+                                          in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0),
+                      slabs[k], "upload");
+                done += m;
+            }
         }
         std::fclose(f);
         int n_out = 0;
-        check(ymflow_flow(ctx, in.epsilon, nsteps, 1, in.reunit_every, obs.data(), int(obs.size()), &n_out), ctx,
-              "flow");
+        if (nslabs == 1)
+            check(ymflow_flow(ctx, in.epsilon, nsteps, 1, in.reunit_every, obs.data(), int(obs.size()), &n_out), ctx,
+                  "flow");
+        else
+            check(ymflow_slab_group_flow(slabs.data(), nslabs, in.epsilon, nsteps, 1, in.reunit_every, obs.data(),
+                                         int(obs.size()), &n_out),
+                  ctx, "flow");
         // OutputTerm::writeObs (outputterm.cpp:58-66) for the configuration as read
         std::printf("Configuration Number %4i\n", conf_num);
         std::printf("\t%s\t = %g \n", "Plaq.", obs[0].plaq);
@@ -262,7 +305,7 @@ int main(int argc, char** argv) {
         conf_num++;
     }
     ymflow_host_free(buf);
-    ymflow_destroy(ctx);
+    for (ymflow_ctx* c : slabs) ymflow_destroy(c);
     const std::chrono::duration<double> el = std::chrono::system_clock::now() - start;
     std::printf("Total time taken: %.2fs\n", el.count());
     return 0;

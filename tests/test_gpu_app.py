@@ -76,6 +76,22 @@ def test_flow_app_big_endian_streamed_input(tmp_path):
         assert (tmp_path / "out" / f).read_bytes() == (exp / f).read_bytes(), f
 
 
+def test_flow_app_time_slabs_from_sublattice_size(tmp_path):
+    """A SubLatticeSize that splits only t flows each configuration as time
+    slabs (here two, on the GPUs present): the same files as the reference
+    application, and its terminal lines apart from the processor count."""
+    run = prepare(tmp_path, {"SubLatticeSize": {"x": 4, "y": 4, "z": 4, "t": 2}})
+    res = subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)
+    got = [l for l in res.stdout.splitlines(keepends=True) if not l.startswith("Total time taken")]
+    exp = (GOLDEN / "app_flow" / "expected" / "stdout.txt").read_text().splitlines(keepends=True)
+    assert "Number of Processors: \t\t2\n" in got and "Number of Active Processors: \t2\n" in got
+    keep = lambda lines: [l for l in lines if not l.startswith(("Number of", "Sublattice Size"))]
+    assert keep(got) == keep(exp)
+    ex = GOLDEN / "app_flow" / "expected"
+    for f in ["observables.dat", "flow/conf0000.dat", "flow/conf0001.dat"]:
+        assert (tmp_path / "out" / f).read_bytes() == (ex / f).read_bytes(), f
+
+
 def test_flow_app_mixed_precision_rows(tmp_path):
     run = prepare(tmp_path, {"Precision": "fp32_12", "ReunitEvery": 5})
     subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)
