@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(128, EnsMinBlocks<F>::value) ens_stage_kernel(
     const int lane_site = ((w >> 2) << 5) + (threadIdx.x & 31);
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const EnsConf& C = confs[find_conf(confs, nconf, item)];
-        const Geo g = C.g;
+        const Geo& g = C.g;
         const int s = (item - C.blk0) * spb + lane_site;
         if (s < g.V) {
             const F in{uin + C.uoff, g.V}, out{uout + C.uoff, g.V};
@@ -68,12 +68,46 @@ __global__ void __launch_bounds__(128, EnsMinBlocks<F>::value) ens_stage_kernel(
     }
 }
 
+// One block per work item (the grid the autotuner picks when every item gets
+// its own block): no item loop, so the kernel keeps the single-configuration
+// kernel's register budget (80 in the FP32 18-real form; the looping kernel
+// spills there).
+template <class F>
+struct EnsFlatMinBlocks {
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : (F::kElems == 9 ? 6 : 5);
+};
+
+template <class F, int STAGE>
+__global__ void __launch_bounds__(128, EnsFlatMinBlocks<F>::value)
+    ens_flat_kernel(char* uin, char* uout, char* z, const EnsConf* __restrict__ confs, int nconf,
+                    typename F::Real eps) {
+    using R = typename F::Real;
+    const int w = threadIdx.x >> 5;
+    const int mu = w & 3;
+    const int item = blockIdx.x;
+    const EnsConf& C = confs[find_conf(confs, nconf, item)];
+    const Geo& g = C.g;  // read where used (L1), not held in registers
+    const int s = (item - C.blk0) * (blockDim.x >> 2) + ((w >> 2) << 5) + (threadIdx.x & 31);
+    if (s >= g.V) return;
+    const F in{uin + C.uoff, g.V}, out{uout + C.uoff, g.V};
+    const ForceField<R> zf{z + C.zoff, g.V};
+    rk_link_update<F, STAGE>(in, out, zf, g, eps, s, mu);
+}
+
 template <class F>
 static cudaError_t launch_ens_typed(int stage, void* uin, void* uout, void* z, const EnsConf* confs, int nconf,
                                     int nitems, int grid, int block, double eps, cudaStream_t st) {
     using R = typename F::Real;
     const R e = R(stage == 0 ? eps * 0.25 : eps);
     char *a = (char*)uin, *b = (char*)uout, *zz = (char*)z;
+    if (grid >= nitems) {
+        switch (stage) {
+            case 0: ens_flat_kernel<F, 0><<<nitems, block, 0, st>>>(a, b, zz, confs, nconf, e); break;
+            case 1: ens_flat_kernel<F, 1><<<nitems, block, 0, st>>>(a, b, zz, confs, nconf, e); break;
+            default: ens_flat_kernel<F, 2><<<nitems, block, 0, st>>>(a, b, zz, confs, nconf, e); break;
+        }
+        return cudaGetLastError();
+    }
     switch (stage) {
         case 0: ens_stage_kernel<F, 0><<<grid, block, 0, st>>>(a, b, zz, confs, nconf, nitems, e); break;
         case 1: ens_stage_kernel<F, 1><<<grid, block, 0, st>>>(a, b, zz, confs, nconf, nitems, e); break;
