@@ -92,6 +92,17 @@ def test_flow_app_time_slabs_from_sublattice_size(tmp_path):
         assert (tmp_path / "out" / f).read_bytes() == (ex / f).read_bytes(), f
 
 
+def test_flow_app_empty_input_dir(tmp_path):
+    """No .bin files: the reference writes its headers and flows nothing."""
+    run = prepare(tmp_path)
+    for f in (tmp_path / "in").glob("*.bin"):
+        f.unlink()
+    res = subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)
+    assert "Configuration Number" not in res.stdout
+    assert (tmp_path / "out" / "observables.dat").read_text() == "Step\tSuperObs\t\n"
+    assert not list((tmp_path / "out" / "flow").glob("*.dat"))
+
+
 def test_flow_app_mixed_precision_rows(tmp_path):
     run = prepare(tmp_path, {"Precision": "fp32_12", "ReunitEvery": 5})
     subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)

@@ -189,3 +189,22 @@ def test_wilsonflow_app_mirror_writes_reference_rows(tmp_path):
     for line, r in zip(lines[1:], ref):
         assert line == "".join("%f\t" % v for v in (r[1], r[2], r[3], r[4]))
     app.field.close()
+
+
+@pytest.mark.parametrize("n", [(1, 2, 3, 4), (2, 2, 2, 2), (1, 1, 1, 6), (5, 1, 2, 3)])
+def test_degenerate_extents_match_oracle(oracle, n):
+    """Extents of 1 (a link is its own neighbour) and 2 (both neighbours are
+    one site): the periodic indexing against the oracle's."""
+    from latticeyangmills_b200 import GluonField
+
+    U = oracle.gen_expiah(n, 0.35, 7, 0)
+    with GluonField(n, "fp64") as f:
+        f.upload(U)
+        rows = f.flow(0.02, 4, 2)
+        got = f.download()
+    want = U.copy()
+    ref = oracle.flow(want, n, 0.02, 4, 2)
+    assert np.abs(got - want).max() < 1e-13
+    np.testing.assert_allclose(rows[:, 2], ref[:, 2], rtol=REL, atol=1e-15)  # plaq
+    np.testing.assert_allclose(rows[:, 4], ref[:, 4], rtol=REL, atol=1e-12)  # energy
+    assert np.abs(rows[:, 3] - ref[:, 3]).max() < 1e-12  # topc
