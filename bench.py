@@ -214,6 +214,23 @@ def host_processes(per_proc_gb: float) -> int:
     return max(1, min(n, 64))
 
 
+def host_cpu() -> dict:
+    """The host's CPU model and usable cores (for the CPU baseline's record)."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count()
+    return {"cpu_model": model, "nproc": cores}
+
+
 def run_reference(dims, nproc: int, steps: int):
     """nproc concurrent single-rank reference processes, each flowing its own copy of
     the seeded configuration `steps` RK3 steps.  Returns (link-updates/s, detail)."""
@@ -254,7 +271,8 @@ def reference_arm(args):
         "data": "synthetic (seeded e^{iaH}, a=0.35)",
         "config": {"workload": "32^4 Wilson flow, RK3 eps=0.01, reference CPU code", "lattice": list(DIMS),
                    "parallelism": "%d host processes" % nproc},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference", "sample": sample,
+                         "host": host_cpu()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -476,7 +494,7 @@ def our_arm(args, dist: Dist):
         if val is not None:
             cpu = {"value": val, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": "one RK3 step of the 32^4 configuration by the reference's own code "
-                             "(oracle/_ref/ref_flow), one core"}
+                             "(oracle/_ref/ref_flow), one core", "host": host_cpu()}
     f.close()
 
     if dist.rank == 0:
