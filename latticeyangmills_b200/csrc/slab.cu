@@ -13,7 +13,8 @@
 //    communicator; ymflow_flow / ymflow_observables then exchange halos with
 //    grouped ncclSend/ncclRecv on the context's stream and sum each
 //    measurement row with ncclAllReduce.  NCCL is loaded at run time
-//    (libnccl.so.2), so the library needs it only when this is used.
+//    (YMFLOW_NCCL_LIB, else the libnccl.so.2 already in the process, else the
+//    loader's), so the library needs it only when this is used.
 //  * Inside one process: ymflow_slab_group_flow flows the slab contexts of one
 //    configuration (on one or several GPUs) stage by stage.  Each slab's stage
 //    kernel also stores its new boundary links straight into its neighbours'
@@ -60,7 +61,14 @@ const NcclApi& nccl() {
     static NcclApi api;
     static std::once_flag once;
     std::call_once(once, [] {
-        void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        // Which NCCL: YMFLOW_NCCL_LIB (a path) first, then one the process has
+        // already loaded (a framework's), then the loader's libnccl.so.2.  A
+        // process must hold one NCCL: a framework imported later binds to the
+        // libnccl.so.2 loaded here, which must then be the one it was built for.
+        void* h = nullptr;
+        if (const char* path = std::getenv("YMFLOW_NCCL_LIB")) h = dlopen(path, RTLD_NOW | RTLD_GLOBAL);
+        if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL | RTLD_NOLOAD);
+        if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
         if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
         if (!h) {
             api.why = "libnccl.so.2 not found";

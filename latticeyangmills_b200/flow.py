@@ -114,6 +114,7 @@ class GluonField:
         0); lower/upper are the ranks holding the neighbouring slices."""
         if len(nccl_id) != N.NCCL_ID_BYTES:
             raise ValueError("an NCCL id has 128 bytes")
+        _prefer_framework_nccl()
         buf = ctypes.create_string_buffer(bytes(nccl_id), N.NCCL_ID_BYTES)
         self._check(N.load().ymflow_slab_connect(self.ctx, buf, int(rank), int(nranks), int(lower), int(upper)))
 
@@ -327,8 +328,26 @@ class Ensemble:
         self._check(N.load().ymflow_ensemble_reset_time(self._ens))
 
 
+def _prefer_framework_nccl() -> None:
+    """Point the library at the NCCL that PyTorch ships (without importing
+    torch), so that torch imported later in this process finds the NCCL it was
+    built against already loaded."""
+    import importlib.util
+    import os
+
+    if os.environ.get("YMFLOW_NCCL_LIB"):
+        return
+    spec = importlib.util.find_spec("nvidia.nccl")
+    for root in (spec.submodule_search_locations or []) if spec else []:
+        lib = Path(root) / "lib" / "libnccl.so.2"
+        if lib.exists():
+            os.environ["YMFLOW_NCCL_LIB"] = str(lib)
+            return
+
+
 def nccl_unique_id() -> bytes:
     """A fresh NCCL communicator id (128 bytes) for GluonField.connect."""
+    _prefer_framework_nccl()
     buf = ctypes.create_string_buffer(N.NCCL_ID_BYTES)
     N.check(N.load().ymflow_nccl_unique_id(buf))
     return buf.raw

@@ -148,3 +148,18 @@ def test_slab_errors():
     finally:
         a.close()
         b.close()
+
+
+def test_nccl_then_torch_in_one_process():
+    """The slab path loads NCCL at run time; torch imported afterwards in the
+    same process must still import (one NCCL, the one torch was built for)."""
+    import subprocess
+    import sys
+
+    code = ("from latticeyangmills_b200 import GluonField, nccl_unique_id\n"
+            "f = GluonField.slab((8, 4, 4, 4), 0, 4, 'fp64'); f.init_links('cold')\n"
+            "f.connect(nccl_unique_id(), 0, 1, 0, 0); f.flow(0.01, 1)\n"
+            "import torch; print('torch', torch.__version__)\n")
+    res = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stderr[-2000:]
+    assert "torch" in res.stdout
