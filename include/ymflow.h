@@ -206,8 +206,11 @@ YMFLOW_API int ymflow_get_option(const ymflow_ctx* ctx, int key, int64_t* value)
  *    ymflow_observables / ymflow_time_steps as usual.  These become collective
  *    over the ranks (every rank calls them with the same arguments).  Halos
  *    travel by NCCL send/recv after every stage; measurement rows are summed
- *    with an NCCL all-reduce.  NCCL (libnccl.so.2) is loaded at run time;
- *    YMFLOW_ERR_NODEVICE if it is missing.
+ *    with an NCCL all-reduce.  NCCL is loaded at run time: the library named
+ *    by YMFLOW_NCCL_LIB, else a libnccl.so.2 the process already holds, else
+ *    the loader's libnccl.so.2 (a process must hold one NCCL: set
+ *    YMFLOW_NCCL_LIB to a framework's copy if that framework is imported
+ *    later); YMFLOW_ERR_NODEVICE if none loads.
  *  - several slabs in one process (one or more GPUs): ymflow_slab_group_flow,
  *    with halos as stream-ordered peer copies.
  * A slab that is neither connected nor flowed through its group returns
