@@ -208,3 +208,29 @@ def test_degenerate_extents_match_oracle(oracle, n):
     np.testing.assert_allclose(rows[:, 2], ref[:, 2], rtol=REL, atol=1e-15)  # plaq
     np.testing.assert_allclose(rows[:, 4], ref[:, 4], rtol=REL, atol=1e-12)  # energy
     assert np.abs(rows[:, 3] - ref[:, 3]).max() < 1e-12  # topc
+
+
+def test_full_size_steps_match_oracle(oracle):
+    """The headline workload itself: 32^4, two RK3 steps, every link and the
+    observables of both rows against the oracle (about 7 s of oracle time)."""
+    from latticeyangmills_b200 import GluonField
+
+    n = (32, 32, 32, 32)
+    U = oracle.gen_expiah(n, 0.35, 20260, 0)
+    want = U.copy()
+    ref = oracle.flow(want, n, 0.01, 2, 2)
+    with GluonField(n, "fp64") as f:
+        f.upload(U)
+        rows = f.flow(0.01, 2, 2)
+        got = f.download()
+    assert np.abs(got - want).max() < 1e-13
+    np.testing.assert_allclose(rows[:, 2], ref[:, 2], rtol=REL, atol=0)
+    np.testing.assert_allclose(rows[:, 4], ref[:, 4], rtol=REL, atol=0)
+    assert np.abs(rows[:, 3] - ref[:, 3]).max() <= topc_tolerance(ref[:, 4].min(), REL)
+    with GluonField(n, "fp32_18") as f:
+        f.upload(U)
+        rows32 = f.flow(0.01, 2, 2)
+        got32 = f.download()
+    assert np.abs(got32 - want).max() < 5e-6
+    np.testing.assert_allclose(rows32[:, 2], ref[:, 2], rtol=1e-6)
+    np.testing.assert_allclose(rows32[:, 4], ref[:, 4], rtol=1e-6)
