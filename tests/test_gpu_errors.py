@@ -83,3 +83,30 @@ def test_fma_peak_is_measured():
     assert 20.0 < tf[N.FP32_18] < 200.0
     assert 5.0 < tf[N.FP64] < tf[N.FP32_18]
     assert N.load().ymflow_fma_peak(0, 7, ctypes.byref(ctypes.c_double())) == N.ERR_ARG
+
+
+def test_pinned_host_buffers_feed_uploads():
+    """ymflow_host_alloc / ymflow_host_free: page-locked staging for uploads."""
+    import ctypes
+
+    import numpy as np
+
+    from latticeyangmills_b200 import GluonField
+    from latticeyangmills_b200 import _native as N
+
+    lib = N.load()
+    p = ctypes.c_void_p()
+    assert lib.ymflow_host_alloc(0, ctypes.byref(p)) == N.ERR_ARG
+    assert lib.ymflow_host_alloc(-5, ctypes.byref(p)) == N.ERR_ARG
+    n = (4, 4, 4, 4)
+    count = 4 * 256 * 18
+    assert lib.ymflow_host_alloc(count * 8, ctypes.byref(p)) == N.OK and p.value
+    buf = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), shape=(count,))
+    with GluonField(n, "fp64") as f:
+        f.init_links("expiah", 0.3, 4)
+        U = f.download()
+        buf[:] = U.reshape(-1)
+        f.init_links("cold")
+        assert lib.ymflow_upload(f.ctx, p) == N.OK
+        assert np.array_equal(f.download(), U)
+    assert lib.ymflow_host_free(p) == N.OK
