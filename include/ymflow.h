@@ -170,6 +170,13 @@ YMFLOW_API int ymflow_su3_exp(const double* q_host, double* r_host, int64_t n, i
 /* Reset the context's step and flow-time counters (a new configuration). */
 YMFLOW_API int ymflow_reset_time(ymflow_ctx* ctx);
 
+/* Set the step and flow-time counters, to resume a flow from a checkpoint:
+ * ymflow_download the links and keep the last row's (step, t); later
+ * ymflow_upload them and set (step, t) to continue with the same rows as an
+ * unbroken flow (the reference keeps no flow checkpoint; its configuration
+ * writer is a no-op, src/InputOutput/outputconf.cpp:102). */
+YMFLOW_API int ymflow_set_time(ymflow_ctx* ctx, int64_t step, double t);
+
 /* Device-timed flow steps for benchmarking: runs nsteps RK3 steps (no
  * measurements) between two CUDA events on the context's stream and writes the
  * elapsed milliseconds.  kernel_ms (optional, may be NULL) receives the summed

@@ -36,7 +36,7 @@ EXPORTS = (
     "ymflow_version", "ymflow_device_count", "ymflow_create", "ymflow_destroy", "ymflow_last_error",
     "ymflow_upload", "ymflow_download", "ymflow_upload_sites", "ymflow_download_sites", "ymflow_init_links",
     "ymflow_generate_metropolis", "ymflow_observables", "ymflow_flow", "ymflow_derivative", "ymflow_su3_exp",
-    "ymflow_reset_time", "ymflow_time_steps", "ymflow_set_option", "ymflow_get_option",
+    "ymflow_reset_time", "ymflow_set_time", "ymflow_time_steps", "ymflow_set_option", "ymflow_get_option",
     "ymflow_host_alloc", "ymflow_host_free", "ymflow_device_bytes", "ymflow_fma_peak",
     "ymflow_ensemble_create", "ymflow_ensemble_destroy", "ymflow_ensemble_last_error",
     "ymflow_ensemble_upload", "ymflow_ensemble_download", "ymflow_ensemble_init_links",
@@ -105,6 +105,7 @@ def load():
     l.ymflow_derivative.argtypes = [vp, ctypes.c_int, vp]
     l.ymflow_su3_exp.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int]
     l.ymflow_reset_time.argtypes = [vp]
+    l.ymflow_set_time.argtypes = [vp, ctypes.c_int64, ctypes.c_double]
     l.ymflow_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                                     ctypes.POINTER(ctypes.c_float)]
     l.ymflow_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_int64]

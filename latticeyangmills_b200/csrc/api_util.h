@@ -1,12 +1,22 @@
 // Host helpers shared by the C-ABI translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 
 #include "ymflow.h"
 
 namespace ym {
+
+// An NVTX range over an ABI call, named after it, so that profiler timelines
+// show the library's work (header-only NVTX v3; free when no tool listens).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Makes `d` current for the scope of a call and restores the caller's device.
 struct DeviceGuard {

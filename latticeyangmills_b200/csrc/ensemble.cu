@@ -499,6 +499,7 @@ int ymflow_ensemble_init_links(ymflow_ens* e, int conf, int kind, double a, uint
 
 int ymflow_ensemble_flow(ymflow_ens* e, double eps, int nsteps, int measure_every, int reunit_every,
                          ymflow_obs* out, int rows_cap, int* n_rows) {
+    NvtxRange range("ymflow_ensemble_flow");
     if (!e) return YMFLOW_ERR_ARG;
     if (n_rows) *n_rows = 0;
     if (nsteps < 0) return efail(e, YMFLOW_ERR_ARG, "nsteps < 0");
@@ -569,6 +570,7 @@ int ymflow_ensemble_flow(ymflow_ens* e, double eps, int nsteps, int measure_ever
 }
 
 int ymflow_ensemble_time_steps(ymflow_ens* e, double eps, int nsteps, float* elapsed_ms) {
+    NvtxRange range("ymflow_ensemble_time_steps");
     if (!e || !elapsed_ms || nsteps < 1) return efail(e, YMFLOW_ERR_ARG, "bad argument to time_steps");
     for (int c = 0; c < e->nconf; c++)
         if (!e->loaded[c]) return efail(e, YMFLOW_ERR_STATE, "configuration not loaded");

@@ -267,6 +267,7 @@ int ymflow_slab_connect(ymflow_ctx* c, const void* id, int rank, int nranks, int
 
 int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nsteps, int measure_every,
                            int reunit_every, ymflow_obs* out, int out_cap, int* n_out) {
+    NvtxRange range("ymflow_slab_group_flow");
     if (n_out) *n_out = 0;
     if (!ctxs || n < 1) return YMFLOW_ERR_ARG;
     for (int i = 0; i < n; i++)

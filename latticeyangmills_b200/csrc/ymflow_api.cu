@@ -379,6 +379,7 @@ int check_site_range(ymflow_ctx* c, const void* p, int64_t first, int64_t n, int
 }  // namespace
 
 int ymflow_upload_sites(ymflow_ctx* c, const double* links, int64_t first_site, int64_t nsites, int flags) {
+    NvtxRange range("ymflow_upload_sites");
     int r = check_site_range(c, links, first_site, nsites, flags);
     if (r != YMFLOW_OK || nsites == 0) return r;
     DeviceGuard guard(c->device);
@@ -397,6 +398,7 @@ int ymflow_upload_sites(ymflow_ctx* c, const double* links, int64_t first_site, 
 }
 
 int ymflow_download_sites(ymflow_ctx* c, double* links, int64_t first_site, int64_t nsites, int flags) {
+    NvtxRange range("ymflow_download_sites");
     int r = check_site_range(c, links, first_site, nsites, flags);
     if (r != YMFLOW_OK) return r;
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
@@ -433,6 +435,7 @@ int ymflow_init_links(ymflow_ctx* c, int kind, double a, uint64_t seed, uint32_t
 
 int ymflow_generate_metropolis(ymflow_ctx* c, int start, double beta, double su3eps, int sweeps, int hits,
                                uint64_t seed, double* acceptance) {
+    NvtxRange range("ymflow_generate_metropolis");
     if (!c) return YMFLOW_ERR_ARG;
     if (c->slab) return fail(c, YMFLOW_ERR_STATE, "generation runs on a whole-lattice context, not a slab");
     if (sweeps < 0 || hits < 1 || !(su3eps > 0.0 && su3eps < 1.0) || !std::isfinite(beta))
@@ -474,6 +477,7 @@ int ymflow_generate_metropolis(ymflow_ctx* c, int start, double beta, double su3
 }
 
 int ymflow_observables(ymflow_ctx* c, ymflow_obs* out) {
+    NvtxRange range("ymflow_observables");
     if (!c || !out) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_observables");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
     DeviceGuard guard(c->device);
@@ -491,6 +495,7 @@ int ymflow_observables(ymflow_ctx* c, ymflow_obs* out) {
 
 int ymflow_flow(ymflow_ctx* c, double eps, int nsteps, int measure_every, int reunit_every, ymflow_obs* out,
                 int out_cap, int* n_out) {
+    NvtxRange range("ymflow_flow");
     if (!c) return YMFLOW_ERR_ARG;
     if (n_out) *n_out = 0;
     if (nsteps < 0 || !std::isfinite(eps)) return fail(c, YMFLOW_ERR_ARG, "nsteps < 0 or eps not finite");
@@ -594,7 +599,16 @@ int ymflow_reset_time(ymflow_ctx* c) {
     return YMFLOW_OK;
 }
 
+int ymflow_set_time(ymflow_ctx* c, int64_t step, double t) {
+    if (!c) return YMFLOW_ERR_ARG;
+    if (step < 0 || !std::isfinite(t)) return fail(c, YMFLOW_ERR_ARG, "step < 0 or t not finite");
+    c->step = step;
+    c->t = t;
+    return YMFLOW_OK;
+}
+
 int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, float* kernel_ms) {
+    NvtxRange range("ymflow_time_steps");
     if (!c || !elapsed_ms || nsteps < 1) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_time_steps");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
     DeviceGuard guard(c->device);

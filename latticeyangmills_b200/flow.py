@@ -225,6 +225,10 @@ class GluonField:
     def reset_time(self) -> None:
         self._check(N.load().ymflow_reset_time(self.ctx))
 
+    def set_time(self, step: int, t: float) -> None:
+        """Resume the step and flow-time counters (after re-uploading a checkpoint)."""
+        self._check(N.load().ymflow_set_time(self.ctx, int(step), float(t)))
+
     def time_steps(self, eps: float, nsteps: int, kernels: bool = False):
         """(elapsed_ms, kernel_ms or None) of nsteps device-timed RK3 steps."""
         el = ctypes.c_float(0)

@@ -110,3 +110,35 @@ def test_pinned_host_buffers_feed_uploads():
         assert lib.ymflow_upload(f.ctx, p) == N.OK
         assert np.array_equal(f.download(), U)
     assert lib.ymflow_host_free(p) == N.OK
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_18"])
+def test_checkpoint_resume_continues_the_flow(precision):
+    """Download mid-flow, upload into a fresh context, set (step, t): the
+    remaining rows and links equal those of an unbroken flow."""
+    import numpy as np
+
+    from latticeyangmills_b200 import GluonField
+
+    n = (8, 8, 8, 8)
+    kw = dict(reunit_every=5) if precision != "fp64" else {}
+    with GluonField(n, precision) as f:
+        f.init_links("expiah", 0.35, 8)
+        whole = f.flow(0.02, 20, 5, **kw)
+        end = f.download()
+    with GluonField(n, precision) as f:
+        f.init_links("expiah", 0.35, 8)
+        first = f.flow(0.02, 10, 5, **kw)
+        ckpt = f.download()
+    with GluonField(n, precision) as g:
+        g.upload(ckpt)
+        g.set_time(int(first[-1, 0]), first[-1, 1])
+        rest = g.flow(0.02, 10, 5, **kw)
+        resumed = g.download()
+    assert np.array_equal(rest[:, :2], whole[2:, :2])  # steps and t continue exactly
+    if precision == "fp64":
+        assert np.array_equal(resumed, end)
+        np.testing.assert_array_equal(rest[:, 2:], whole[2:, 2:])
+    else:  # the checkpoint passes through the FP64 .bin layout: equal to FP32 rounding of that round trip
+        assert np.abs(resumed - end).max() < 1e-5
+        np.testing.assert_allclose(rest[:, 2:], whole[2:, 2:], rtol=1e-5)

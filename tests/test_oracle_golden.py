@@ -9,7 +9,7 @@ import json
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, case_field, load_case
+from conftest import GOLDEN, ROOT, case_field, load_case
 
 BITWISE_CASES = ["g4_expiah", "g3456_expiah", "g2324_expiah", "g8_metropolis", "g8_haar"]
 
@@ -138,3 +138,19 @@ def test_checkerboard_chain_properties(oracle):
     assert 0.08 < acc / (40 * 10 * 4 * V) < 0.2
     assert 0.55 < plaq < 0.7
     assert max(oracle.unitarity(c)) < 1e-12
+
+
+def test_oracle_clean_under_sanitizers():
+    """Every oracle entry point on odd and degenerate lattices under
+    AddressSanitizer and UndefinedBehaviorSanitizer (oracle/sanitize_driver.c)."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    res = subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "sanitize"], capture_output=True, text=True,
+                         timeout=600)
+    if res.returncode != 0 and "cannot find" in res.stderr and "asan" in res.stderr:
+        pytest.skip("no sanitizer runtime")
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+    assert "sanitize ok" in res.stdout
