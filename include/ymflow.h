@@ -110,6 +110,14 @@ YMFLOW_API int ymflow_download(ymflow_ctx* ctx, double* links_aos);
  * every site before flowing.  Synchronous like ymflow_upload/ymflow_download;
  * the device staging buffer grows to the largest range used. */
 #define YMFLOW_IO_BIG_ENDIAN 1
+
+/* Load a .bin configuration file into the context (its part of it, for a
+ * slab): the file is read in chunks of chunk_sites sites (0: 65536) through two
+ * pinned buffers, the read of one chunk overlapping the copy and unpacking of
+ * the one before, so a 64^4 file (9.7 GB) loads at disk speed with no
+ * whole-field host copy.  flags as for ymflow_upload_sites; YMFLOW_ERR_ARG if
+ * the file's size is not the configuration's. */
+YMFLOW_API int ymflow_load_file(ymflow_ctx* ctx, const char* path, int flags, int64_t chunk_sites);
 YMFLOW_API int ymflow_upload_sites(ymflow_ctx* ctx, const double* links_aos, int64_t first_site, int64_t nsites,
                                    int flags);
 YMFLOW_API int ymflow_download_sites(ymflow_ctx* ctx, double* links_aos, int64_t first_site, int64_t nsites,

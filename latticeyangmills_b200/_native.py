@@ -34,7 +34,8 @@ OPT_BLOCK, OPT_GRAPH, OPT_OBS_BLOCK = 1, 2, 3
 # every symbol include/ymflow.h declares
 EXPORTS = (
     "ymflow_version", "ymflow_device_count", "ymflow_create", "ymflow_destroy", "ymflow_last_error",
-    "ymflow_upload", "ymflow_download", "ymflow_upload_sites", "ymflow_download_sites", "ymflow_init_links",
+    "ymflow_upload", "ymflow_download", "ymflow_upload_sites", "ymflow_download_sites", "ymflow_load_file",
+    "ymflow_init_links",
     "ymflow_generate_metropolis", "ymflow_observables", "ymflow_flow", "ymflow_derivative", "ymflow_su3_exp",
     "ymflow_reset_time", "ymflow_set_time", "ymflow_time_steps", "ymflow_set_option", "ymflow_get_option",
     "ymflow_host_alloc", "ymflow_host_free", "ymflow_device_bytes", "ymflow_fma_peak",
@@ -96,6 +97,7 @@ def load():
                                     ctypes.c_double]
     l.ymflow_observables.argtypes = [vp, ctypes.POINTER(Obs)]
     l.ymflow_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    l.ymflow_load_file.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int64]
     l.ymflow_upload_sites.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
     l.ymflow_download_sites.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
     l.ymflow_generate_metropolis.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,

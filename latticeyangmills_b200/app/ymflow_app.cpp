@@ -16,9 +16,10 @@
 // "FOR CHROMA" reader, inputconf.cpp:135-143), "IOChunkSites" (sites per
 // streamed read, default 65536).
 //
-// Configurations are streamed: each file is read in chunks into one pinned
-// buffer and uploaded range by range (byte reversal on the device), so no
-// whole-field host copy is held (a 64^4 .bin is 9.7 GB).
+// Configurations are streamed: ymflow_load_file reads each file in chunks
+// through two pinned buffers, overlapping the reads with the device copies
+// (byte reversal on the device), so no whole-field host copy is held (a 64^4
+// .bin is 9.7 GB).
 //
 // Same inputs and outputs: every *.bin in InputDir in sorted order
 // (inputconf.cpp:76-82), int(tauFinal/epsilon) rows per configuration with
@@ -225,41 +226,16 @@ int main(int argc, char** argv) {
         }
     }
     ymflow_ctx* ctx = slabs[0];
-    const int64_t slab_sites = int64_t(in.size[0]) * in.size[1] * in.size[2] * (nslabs > 1 ? in.sub[3] : in.size[3]);
 
-    const int64_t V = int64_t(in.size[0]) * in.size[1] * in.size[2] * in.size[3];
-    const int64_t chunk = std::min<int64_t>(in.chunk_sites, V);
-    void* pinned = nullptr;
-    if (ymflow_host_alloc(chunk * 72 * int64_t(sizeof(double)), &pinned) != YMFLOW_OK || !pinned)
-        die("cannot allocate the pinned read buffer");
-    double* buf = static_cast<double*>(pinned);
     const int rows = int(in.tau_final / in.epsilon);  // wilsonflow.cpp:117
     const int nsteps = rows > 1 ? rows - 1 : 0;
     std::vector<ymflow_obs> obs(size_t(nsteps) + 2);
 
     int conf_num = 0;
     for (const std::string& path : input_list(in.input_dir)) {
-        FILE* f = std::fopen(path.c_str(), "rb");
-        if (!f) die("cannot open " + path);
-        for (int64_t first = 0; first < V; first += chunk) {
-            const int64_t n = std::min(chunk, V - first);
-            const size_t want = size_t(n) * 72;
-            if (std::fread(buf, sizeof(double), want, f) != want) {
-                std::fclose(f);
-                die(path + ": shorter than the LatticeSize configuration");
-            }
-            // the chunk's sites, slab by slab (each slab holds a contiguous range of the file)
-            for (int64_t done = 0; done < n;) {
-                const int64_t site = first + done;
-                const int k = int(site / slab_sites);
-                const int64_t m = std::min(n - done, (k + 1) * slab_sites - site);
-                check(ymflow_upload_sites(slabs[k], buf + done * 72, site - k * slab_sites, m,
-                                          in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0),
-                      slabs[k], "upload");
-                done += m;
-            }
-        }
-        std::fclose(f);
+        for (ymflow_ctx* c : slabs)  // each slab reads its own part of the file
+            check(ymflow_load_file(c, path.c_str(), in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0, in.chunk_sites), c,
+                  "load");
         int n_out = 0;
         if (nslabs == 1)
             check(ymflow_flow(ctx, in.epsilon, nsteps, 1, in.reunit_every, obs.data(), int(obs.size()), &n_out), ctx,
@@ -304,7 +280,6 @@ int main(int argc, char** argv) {
         }
         conf_num++;
     }
-    ymflow_host_free(buf);
     for (ymflow_ctx* c : slabs) ymflow_destroy(c);
     const std::chrono::duration<double> el = std::chrono::system_clock::now() - start;
     std::printf("Total time taken: %.2fs\n", el.count());

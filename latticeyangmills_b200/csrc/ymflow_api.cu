@@ -4,6 +4,7 @@
 // (src/Apps/wilsonflow.cpp:115-136).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -377,6 +378,73 @@ int check_site_range(ymflow_ctx* c, const void* p, int64_t first, int64_t n, int
 }
 
 }  // namespace
+
+int ymflow_load_file(ymflow_ctx* c, const char* path, int flags, int64_t chunk_sites) {
+    NvtxRange range("ymflow_load_file");
+    if (!c || !path) return YMFLOW_ERR_ARG;
+    if (flags & ~YMFLOW_IO_BIG_ENDIAN) return fail(c, YMFLOW_ERR_ARG, "unknown flags");
+    const int64_t n = c->geo.site1 - c->geo.site0;  // this context's sites
+    const int64_t site_bytes = 4 * 18 * int64_t(sizeof(double));
+    const int64_t chunk = std::min<int64_t>(chunk_sites > 0 ? chunk_sites : 65536, n);
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(c, YMFLOW_ERR_ARG, std::string("cannot open ") + path);
+    std::fseek(f, 0, SEEK_END);
+    const int64_t file_bytes = std::ftell(f);
+    if (file_bytes != c->geo.vglobal * site_bytes) {
+        std::fclose(f);
+        return fail(c, YMFLOW_ERR_ARG, std::string(path) + ": " + std::to_string(file_bytes) + " bytes, expected " +
+                                           std::to_string(c->geo.vglobal * site_bytes));
+    }
+    std::fseek(f, long(c->geo.global0 * site_bytes), SEEK_SET);  // a slab's part starts at its first site
+    DeviceGuard guard(c->device);
+    int r = ensure_staging(c, size_t(2 * chunk * site_bytes));
+    double* pinned[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    auto cleanup = [&]() {
+        for (int i = 0; i < 2; i++) {
+            if (done[i]) cudaEventDestroy(done[i]);
+            if (pinned[i]) cudaFreeHost(pinned[i]);
+        }
+        std::fclose(f);
+    };
+    for (int i = 0; i < 2 && r == YMFLOW_OK; i++) {
+        cudaError_t e = cudaMallocHost((void**)&pinned[i], size_t(chunk * site_bytes));
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+        if (e != cudaSuccess) r = cuda_fail(c, e, "pinned read buffers");
+    }
+    // Double buffering: the host reads chunk k+1 from the file while the device
+    // copies and packs chunk k; a buffer is refilled once its copy has completed.
+    for (int64_t first = 0, k = 0; first < n && r == YMFLOW_OK; first += chunk, k++) {
+        const int b = int(k & 1);
+        const int64_t m = std::min(chunk, n - first);
+        cudaError_t e = cudaEventSynchronize(done[b]);
+        if (e != cudaSuccess) {
+            r = cuda_fail(c, e, "read buffer wait");
+            break;
+        }
+        if (std::fread(pinned[b], size_t(site_bytes), size_t(m), f) != size_t(m)) {
+            r = fail(c, YMFLOW_ERR_ARG, std::string(path) + ": short read");
+            break;
+        }
+        double* dst = c->staging + size_t(b) * size_t(chunk) * 72;
+        e = cudaMemcpyAsync(dst, pinned[b], size_t(m * site_bytes), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(done[b], c->stream);
+        if (e == cudaSuccess)
+            e = launch_pack_range(c->prec, dst, c->u[c->cur], c->geo, c->geo.site0 + int(first), int(m),
+                                  (flags & YMFLOW_IO_BIG_ENDIAN) != 0, c->stream);
+        if (e != cudaSuccess) r = cuda_fail(c, e, "load copy");
+    }
+    if (r == YMFLOW_OK) {
+        const cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) r = cuda_fail(c, e, "load");
+    }
+    cleanup();
+    if (r != YMFLOW_OK) return r;
+    c->loaded = true;
+    c->step = 0;
+    c->t = 0.0;
+    return YMFLOW_OK;
+}
 
 int ymflow_upload_sites(ymflow_ctx* c, const double* links, int64_t first_site, int64_t nsites, int flags) {
     NvtxRange range("ymflow_upload_sites");

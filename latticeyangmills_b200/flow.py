@@ -173,16 +173,10 @@ class GluonField:
         return a
 
     def load_conf(self, path, big_endian: bool = False, chunk_sites: int = 65536) -> None:
-        """Streams a .bin file into the field chunk by chunk (no whole-field host copy)."""
-        V = self.sites
-        size = Path(path).stat().st_size
-        if size != V * 72 * 8:
-            raise ValueError(f"{path}: {size} bytes, expected {V * 72 * 8}")
-        dt = ">f8" if big_endian else "<f8"
-        with open(path, "rb") as fh:
-            for first in range(0, V, chunk_sites):
-                n = min(chunk_sites, V - first)
-                self.upload_sites(np.fromfile(fh, dtype=dt, count=n * 72), first)
+        """Loads a .bin file (this context's part of it, for a slab) through the
+        library's double-buffered reader: no whole-field host copy."""
+        flags = N.IO_BIG_ENDIAN if big_endian else 0
+        self._check(N.load().ymflow_load_file(self.ctx, str(path).encode(), flags, int(chunk_sites)))
 
     def init_links(self, kind: str = "expiah", a: float = 0.35, seed: int = 1, config: int = 0,
                    haar_frac: float = 0.0) -> None:

@@ -78,3 +78,28 @@ def test_ranges_are_checked():
             f.upload_sites(U[:10], -1)
         assert load().ymflow_upload_sites(f.ctx, U.ctypes.data, 0, 1, 2) != 0
         f.upload_sites(U[:0], 0)  # empty range: no-op
+
+
+def test_load_file_slabs_and_errors(tmp_path):
+    """ymflow_load_file: each slab reads only its part of the file; a file of
+    the wrong size is refused."""
+    from latticeyangmills_b200 import GluonField, YmflowError, write_conf
+
+    n = (8, 4, 4, 6)
+    U = field6 = np.random.default_rng(3).standard_normal((n[3], n[2], n[1], n[0], 4, 18))
+    write_conf(tmp_path / "c.bin", U)
+    with GluonField(n, "fp64") as f:
+        f.load_conf(tmp_path / "c.bin", chunk_sites=50)
+        assert np.array_equal(f.download(), U)
+    parts = []
+    for t0, nt in ((0, 2), (2, 3), (5, 1)):
+        with GluonField.slab(n, t0, nt, "fp64") as s:
+            s.load_conf(tmp_path / "c.bin", chunk_sites=40)
+            parts.append(s.download())
+    assert np.array_equal(np.concatenate(parts), field6)
+    (tmp_path / "short.bin").write_bytes((tmp_path / "c.bin").read_bytes()[:-8])
+    with GluonField(n, "fp64") as f:
+        with pytest.raises(YmflowError):
+            f.load_conf(tmp_path / "short.bin")
+        with pytest.raises(YmflowError):
+            f.load_conf(tmp_path / "missing.bin")
