@@ -62,6 +62,20 @@ struct Geo {
     // indices), vglobal the configuration's volume (normalisations).
     int site0, site1;
     long long global0, vglobal;
+    // Block order of the stage kernel (one 32-site group per block): 0 = plain;
+    // otherwise the time coordinate advances every tile_groups blocks, so a
+    // link read as a time neighbour is read again a few hundred blocks later,
+    // still in L2 (tile_groups divides slice_groups, the groups per time slice).
+    int slice_groups, tile_groups;
+
+    __device__ __forceinline__ int block_group(int b) const {
+        if (tile_groups == 0) return b;
+        const int per_tile = tile_groups * n[3];
+        const int ti = b / per_tile;
+        const int r = b - ti * per_tile;
+        const int t = r / tile_groups;
+        return t * slice_groups + ti * tile_groups + (r - t * tile_groups);
+    }
 
     __device__ __forceinline__ static int fdiv(int x, const FastDiv& f) {
         return int((uint64_t(uint32_t(x)) * f.m) >> (32 + f.l));
@@ -113,7 +127,22 @@ inline Geo make_geo(const int dims[4]) {
     g.site1 = g.V;
     g.global0 = 0;
     g.vglobal = g.V;
+    const int vs = dims[0] * dims[1] * dims[2];
+    g.slice_groups = vs % 32 == 0 ? vs / 32 : 0;
+    g.tile_groups = 0;
     return g;
+}
+
+// The tiled block order with tiles of about `target` groups (a divisor of the
+// groups per time slice), where the slices hold more than `target` groups.
+inline void set_tiled_order(Geo& g, int target) {
+    g.tile_groups = 0;
+    if (g.slice_groups <= target || g.site0 != 0 || g.site1 != g.V) return;
+    for (int t = target; t >= target / 4; t--)
+        if (g.slice_groups % t == 0) {
+            g.tile_groups = t;
+            return;
+        }
 }
 
 inline int64_t padded_sites(int64_t V) { return (V + 31) & ~int64_t(31); }

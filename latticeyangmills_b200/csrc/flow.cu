@@ -10,10 +10,14 @@ namespace ym {
 // mu = w & 3 for 32 consecutive sites, so the four directions of a site range
 // run side by side and share their neighbour links through L1/L2 (a grid that
 // sweeps all sites once per direction streams the field through L2 four times).
+// TILED: the block order of Geo::block_group (FP64 stage kernels); otherwise
+// blocks take consecutive groups.
+template <bool TILED>
 __device__ __forceinline__ void link_of_thread(const Geo& g, int& s, int& mu) {
     const int w = threadIdx.x >> 5;
     mu = w & 3;
-    s = g.site0 + int(blockIdx.x) * (blockDim.x >> 2) + ((w >> 2) << 5) + (threadIdx.x & 31);
+    const int b = TILED ? g.block_group(int(blockIdx.x)) : int(blockIdx.x);
+    s = g.site0 + b * 32 + (threadIdx.x & 31);  // 128 threads: one 32-site group per block
 }
 
 // Resident 128-thread blocks per SM the stage kernel is compiled for (caps its
@@ -31,7 +35,7 @@ __global__ void __launch_bounds__(128, StageMinBlocks<F>::value)
     rk_stage_kernel(F in, F out, ForceField<typename F::Real> zf, Geo g, typename F::Real eps) {
     int s;
     int mu;
-    link_of_thread(g, s, mu);
+    link_of_thread<sizeof(typename F::Real) == 8>(g, s, mu);
     if (s >= g.site1) return;
     rk_link_update<F, STAGE>(in, out, zf, g, eps, s, mu);
 }
@@ -44,7 +48,7 @@ __global__ void __launch_bounds__(128, StageMinBlocks<F>::value)
                          HaloTargets<F> h) {
     int s;
     int mu;
-    link_of_thread(g, s, mu);
+    link_of_thread<false>(g, s, mu);  // slabs: plain order
     if (s >= g.site1) return;
     rk_link_update_to<F, STAGE, true>(in, out, zf, g, eps, s, mu, h);
 }

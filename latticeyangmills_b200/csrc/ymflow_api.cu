@@ -271,6 +271,11 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     c->prec = precision;
     for (int i = 0; i < 4; i++) c->dims[i] = dims[i];
     c->geo = make_geo(dims);
+    // FP64 re-reads time-neighbour links from DRAM (traffic 1.3x the compulsory
+    // bytes); a tiled block order keeps them in L2: 3 % faster at 32^4.  Only
+    // the FP64 stage kernels use it: the FP32 forms' working set already fits
+    // L2, and they lose 3 % with it.
+    set_tiled_order(c->geo, 512);
     int r = YMFLOW_OK;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) r = YMFLOW_ERR_CUDA;
     const size_t ub = link_field_bytes(c->prec, V);
@@ -323,6 +328,7 @@ ymflow_ctx* ymflow_create_slab(const int global_dims[4], int t0, int nt, int pre
     ymflow_ctx* c = ymflow_create(local, precision, device, status);
     if (!c) return nullptr;
     c->slab = true;
+    c->geo.tile_groups = 0;  // the interior range starts at a halo slice: plain order
     c->t0 = t0;
     c->nt = nt;
     for (int i = 0; i < 4; i++) c->gdims[i] = global_dims[i];
