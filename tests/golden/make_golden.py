@@ -38,6 +38,8 @@ CASES = [
     ("g8_haar", (8, 8, 8, 8), {"kind": "expiah_haar", "a": 0.35, "seed": 5, "haar_frac": 0.05},
      (0.02, 20, 5), False),
     ("g16x32_expiah", (16, 16, 16, 32), {"kind": "expiah", "a": 0.35, "seed": 4}, (0.01, 10, 5), False),
+    # configuration 2 at full length (about 15 min of the reference on one core)
+    ("g16x32_full", (16, 16, 16, 32), {"kind": "expiah", "a": 0.35, "seed": 4}, (0.01, 200, 10), False),
     ("g4_cold", (4, 4, 4, 4), {"kind": "cold"}, (0.01, 2, 1), False),
 ]
 

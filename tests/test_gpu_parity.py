@@ -11,7 +11,7 @@ from conftest import GOLDEN, case_field, load_case, topc_tolerance
 pytestmark = pytest.mark.gpu
 
 REL = 1e-12  # relative tolerance on plaq, energy and t^2<E> (FP64 path)
-CASES = ["g4_expiah", "g3456_expiah", "g2324_expiah", "g8_metropolis", "g8_haar", "g16x32_expiah"]
+CASES = ["g4_expiah", "g3456_expiah", "g2324_expiah", "g8_metropolis", "g8_haar", "g16x32_expiah", "g16x32_full"]
 
 
 def run_case(name, precision="fp64"):
