@@ -71,10 +71,11 @@ typedef struct {
     double t2E;     /* t^2 <E> = -t^2 energy / (64 V) */
 } ymflow_obs;
 
-/* Library version string. */
+/* Library version string (no counterpart in the reference). */
 YMFLOW_API const char* ymflow_version(void);
 
-/* Number of usable (sm_100) CUDA devices. */
+/* Number of usable (sm_100) CUDA devices; the reference's rank count comes from
+ * MPI instead (src/ParallelTools/parallel.cpp:57-70). */
 YMFLOW_API int ymflow_device_count(int* count);
 
 /* Create a flow context for a dims[0] x dims[1] x dims[2] x dims[3] periodic
@@ -233,18 +234,22 @@ YMFLOW_API int ymflow_get_option(const ymflow_ctx* ctx, int key, int64_t* value)
 YMFLOW_API ymflow_ctx* ymflow_create_slab(const int global_dims[4], int t0, int nt, int precision, int device,
                                           int* status);
 
-/* NCCL communicator set-up: rank 0 makes the id and shares its bytes with the
- * other ranks (e.g. through torch.distributed); every rank then connects its
- * slab, naming the ranks that hold the slices below t0 and above t0 + nt - 1
- * (periodically; a single rank is its own neighbour). */
+/* NCCL communicator set-up, in place of the reference's MPI Cartesian
+ * communicator and neighbour ranks (src/ParallelTools/parallel.cpp:72-100):
+ * rank 0 makes the id and shares its bytes with the other ranks (e.g. through
+ * torch.distributed); every rank then connects its slab, naming the ranks that
+ * hold the slices below t0 and above t0 + nt - 1 (periodically; a single rank
+ * is its own neighbour). */
 #define YMFLOW_NCCL_ID_BYTES 128
 YMFLOW_API int ymflow_nccl_unique_id(void* id);
 YMFLOW_API int ymflow_slab_connect(ymflow_ctx* ctx, const void* id, int rank, int nranks, int lower_rank,
                                    int upper_rank);
 
 /* ymflow_flow over the n slab contexts of one configuration, in time order
- * (ctxs[i] starts where ctxs[i-1] ends), held in this process.  Rows as
- * ymflow_flow's, for the whole configuration. */
+ * (ctxs[i] starts where ctxs[i-1] ends), held in this process: the reference's
+ * flow on a decomposed lattice (WilsonFlow::flowStep with shift()'s face
+ * exchange, src/Apps/wilsonflow.cpp:141-172, include/Math/lattice.h:437-449).
+ * Rows as ymflow_flow's, for the whole configuration. */
 YMFLOW_API int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nsteps, int measure_every,
                                       int reunit_every, ymflow_obs* out, int out_cap, int* n_out);
 
