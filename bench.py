@@ -19,6 +19,15 @@ timing is the max over ranks, `value` the sum of all ranks' link-updates.
 --decompose times one configuration split into N time slabs, one per rank,
 with halos exchanged by NCCL after every stage (strong scaling).  At N = 1
 the single slab exchanges with itself, which prices the exchange on one GPU.
+
+  python bench.py --workload 8 | 16x32 | 64   # the other configurations, every precision against FP64
+  python bench.py --profile [--profile-kernel obs] --precision P   # only the timed kernels, for ncu
+
+The JSON line carries, besides the contract's keys: `roofline` (HBM, the
+stage kernel's algorithmic bytes over its event-timed launches), `alu_roofline`
+(the same launches against the measured FP32 or FP64 FMA peak),
+`accuracy_vs_fp64` (t^2 E and Q at t = 4), `ensemble` (64 configurations of
+four sizes) and `cpu_baseline` (the reference's own code on one host core).
 """
 from __future__ import annotations
 
