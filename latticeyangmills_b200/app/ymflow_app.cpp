@@ -1,5 +1,5 @@
 // ymflow_flow — drop-in replacement for the reference's LatticeQCD binary run
-// with a FLOW input file (src/MainPrograms/LatticeQCDMain.cpp:5-30), on one B200.
+// with a FLOW or PGFG input file (src/MainPrograms/LatticeQCDMain.cpp:5-30), on B200s.
 //
 //   ymflow_flow input.json
 //
@@ -36,6 +36,25 @@
 // B200s present from "Device"), with the halo exchange inside the stage kernel
 // (ymflow_slab_group_flow).  Any other SubLatticeSize is validated and the
 // lattice flows whole on one GPU.
+//
+// PGFG (the reference's gauge-field generator, src/Apps/gaugefieldfactory.cpp,
+// whose update does not compile): the same App keys and validation
+// (jsonapp.cpp:66-88, 103-118),
+//   "App": {"type": "PGFG", "params": {"startType": "Cold"|"Hot", "MCSteps": M,
+//           "thermSteps": T, "SU3eps": e, "NConf": n  or  "NCorr": c}}
+// with NConf = MCSteps / NCorr when NCorr is given and MCSteps / NConf sweeps
+// between configurations (gaugefieldfactory.cpp constructor), the same loops:
+// thermSteps sweeps with a report every MCSteps / NConf, then MCSteps sweeps
+// saving OutputDir/confNNNN.bin (outputconf.cpp:89-91, the .bin layout the FLOW
+// app reads) and appending to OutputDir/observables.dat at each multiple of
+// MCSteps / NConf (gaugefieldfactory.cpp:97-130).  The sweeps run on the device
+// (ymflow_generate_metropolis: checkerboard Metropolis of the action's beta,
+// 30 hits per link as gaugefieldfactory.cpp:210, seeded).  The reference prints
+// and writes Observable::value(), which SuperObs leaves 0 (superobs.cpp:32);
+// these lines and rows carry SuperObs' plaquette, charge and energy instead,
+// and OutputDir/observables.full.dat repeats them at full precision with the
+// acceptance.  "Hot" is Haar-random SU(3).  Optional keys: "Seed" (default 1),
+// "MetropolisHits" (default 30).  InputDir is not read (jsondirectories.cpp:20-31).
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -61,7 +80,13 @@ namespace {
 }
 
 struct Input {
+    bool generate = false;  // App "PGFG" (else "FLOW")
     double epsilon = 0.0, tau_final = 0.0, beta = 0.0;
+    // PGFG
+    int mc_steps = 0, therm_steps = 0, corr_steps = 0, hits = 30;
+    double su3eps = 0.0;
+    bool hot = false, measure = false;
+    uint64_t seed = 1;
     int size[4] = {0, 0, 0, 0};
     int sub[4] = {0, 0, 0, 0};
     std::string input_dir, output_dir;
@@ -102,17 +127,48 @@ Input parse_input(const char* path) {
     const jl::Value& app = root["App"];
     if (app["type"].size() == 0) die("no App specified");
     if (app["type"].size() != 1) die("wrong App specification");
-    if (!app["type"].is_string("FLOW")) {
-        if (app["type"].is_string("GFR") || app["type"].is_string("PGFG"))
-            die("App \"" + app["type"].str + "\" is not part of this drop-in; only \"FLOW\" is provided");
+    const jl::Value& params = app["params"];
+    if (app["type"].is_string("PGFG")) {
+        in.generate = true;
+        if (params.size() != 5 || params["startType"].size() != 1 || params["MCSteps"].size() != 1 ||
+            params["thermSteps"].size() != 1 || params["SU3eps"].size() != 1 ||
+            params["NConf"].size() + params["NCorr"].size() != 1)
+            die("wrong \"PGFG\" app specification\nCorrect format:\"App\" : {\n   \"type\" : \"PGFG\", \n"
+                "   \"params\" : { \n       \"MCSteps\"   :  MCSteps, \n       \"themSteps\" :  thermSteps\n"
+                "       \"startType\" :  startType, \n       \"NConf\"     : NConf,   OR    \"NCorr\" : NCorr, \n"
+                "       \"SU3eps\"    : SU3eps \n   }\n}");
+        const std::string start = params["startType"].kind == jl::Value::String ? params["startType"].str : "";
+        if (start != "Cold" && start != "Hot") die("startType must be \"Cold\" or \"Hot\"");
+        in.hot = start == "Hot";
+        in.mc_steps = int(params["MCSteps"].num);
+        in.therm_steps = int(params["thermSteps"].num);
+        in.su3eps = params["SU3eps"].num;
+        // registerPGFG (jsonapp.cpp:103-118) and the GaugeFieldFactory constructor
+        int nconf = 0;
+        if (params["NConf"].size() == 1) {
+            nconf = int(params["NConf"].num);
+        } else {
+            const int ncorr = int(params["NCorr"].num);
+            if (ncorr < 1) die("NCorr must be >= 1");
+            nconf = in.mc_steps / ncorr;
+        }
+        if (in.mc_steps < 1 || in.therm_steps < 0) die("need MCSteps >= 1 and thermSteps >= 0");
+        if (nconf < 1 || in.mc_steps / nconf < 1) die("need 1 <= NConf <= MCSteps");
+        in.corr_steps = in.mc_steps / nconf;
+        if (!(in.su3eps > 0.0 && in.su3eps < 1.0)) die("SU3eps must lie in (0, 1)");
+    } else if (app["type"].is_string("FLOW")) {
+        if (params.size() != 2 || params["epsilon"].size() != 1 || params["tauFinal"].size() != 1)
+            die("wrong \"FLOW\" app specification\nCorrect format:\"App\" : {\n   \"type\" : \"FLOW\", \n"
+                "   \"params\" : { \n       \"epsilon\" : epsilon, \n       \"tauFinal\" : tauFinal \n   }\n}");
+        in.epsilon = params["epsilon"].num;
+        in.tau_final = params["tauFinal"].num;
+        if (!(in.epsilon > 0.0) || !(in.tau_final >= 0.0)) die("epsilon must be > 0 and tauFinal >= 0");
+    } else if (app["type"].is_string("GFR")) {
+        die("App \"GFR\" is not part of this drop-in (the reference's GaugeFieldReader::navigateConf is empty); "
+            "\"FLOW\" and \"PGFG\" are provided");
+    } else {
         die("unknown App " + (app["type"].kind == jl::Value::String ? app["type"].str : std::string("?")));
     }
-    const jl::Value& params = app["params"];
-    if (params.size() != 2 || params["epsilon"].size() != 1 || params["tauFinal"].size() != 1)
-        die("wrong \"FLOW\" app specification\nCorrect format:\"App\" : {\n   \"type\" : \"FLOW\", \n"
-            "   \"params\" : { \n       \"epsilon\" : epsilon, \n       \"tauFinal\" : tauFinal \n   }\n}");
-    in.epsilon = params["epsilon"].num;
-    in.tau_final = params["tauFinal"].num;
     // lattice (jsonlattice.cpp:11-73)
     read_extents(root, "LatticeSize", in.size);
     read_extents(root, "SubLatticeSize", in.sub);
@@ -133,11 +189,12 @@ Input parse_input(const char* path) {
             die("unknown Observable \"" + s + "\"");
         superobs = superobs || s == "superobs";
     }
-    if (!superobs) die("FLOW measures through \"superobs\"; add it to Observables");
-    // directories (jsondirectories.cpp:20-55)
-    if (root.count("InputDir") == 0) die("no InputDir specified");
+    if (!superobs && !in.generate) die("FLOW measures through \"superobs\"; add it to Observables");
+    in.measure = superobs;  // the reference registers only "superobs" (jsonobservable.cpp:64-78)
+    // directories (jsondirectories.cpp:20-55); the generator reads no InputDir
+    if (!in.generate && root.count("InputDir") == 0) die("no InputDir specified");
     if (root.count("OutputDir") == 0) die("no OutputDir specified");
-    in.input_dir = root["InputDir"].str;
+    if (!in.generate) in.input_dir = root["InputDir"].str;
     in.output_dir = root["OutputDir"].str;
     // additions
     if (root.count("Precision")) {
@@ -158,7 +215,14 @@ Input parse_input(const char* path) {
         in.chunk_sites = int64_t(root["IOChunkSites"].num);
         if (in.chunk_sites < 1) die("IOChunkSites must be >= 1");
     }
-    if (!(in.epsilon > 0.0) || !(in.tau_final >= 0.0)) die("epsilon must be > 0 and tauFinal >= 0");
+    if (root.count("Seed")) {
+        if (root["Seed"].kind != jl::Value::Number || root["Seed"].num < 0) die("Seed must be a number >= 0");
+        in.seed = uint64_t(root["Seed"].num);
+    }
+    if (root.count("MetropolisHits")) {
+        in.hits = int(root["MetropolisHits"].num);
+        if (in.hits < 1) die("MetropolisHits must be >= 1");
+    }
     return in;
 }
 
@@ -179,6 +243,101 @@ void check(int st, ymflow_ctx* ctx, const char* what) {
     if (st != YMFLOW_OK) die(std::string(what) + ": " + ymflow_last_error(ctx) + " (status " + std::to_string(st) + ")");
 }
 
+// OutputDir/confNNNN.bin (OutputConf::writeConf, outputconf.cpp:80-104, whose
+// write is commented out): the links in the .bin layout the FLOW app reads,
+// streamed from the device in chunks of IOChunkSites sites.
+void write_conf(ymflow_ctx* ctx, const Input& in, int conf_num) {
+    char name[1024];
+    std::snprintf(name, sizeof(name), "%s/conf%04d.bin", in.output_dir.c_str(), conf_num);
+    FILE* f = std::fopen(name, "wb");
+    if (!f) die(std::string("cannot write ") + name);
+    const int64_t vol = int64_t(in.size[0]) * in.size[1] * in.size[2] * in.size[3];
+    const int64_t chunk = std::min<int64_t>(in.chunk_sites, vol);
+    std::vector<double> buf(static_cast<size_t>(chunk) * 72);
+    for (int64_t s = 0; s < vol; s += chunk) {
+        const int64_t n = std::min(chunk, vol - s);
+        check(ymflow_download_sites(ctx, buf.data(), s, n, in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0), ctx,
+              "download");
+        if (std::fwrite(buf.data(), sizeof(double) * 72, size_t(n), f) != size_t(n))
+            die(std::string("short write to ") + name);
+    }
+    if (std::fclose(f) != 0) die(std::string("cannot close ") + name);
+}
+
+// The PGFG application: GaugeFieldFactory::execute (gaugefieldfactory.cpp:62-108,
+// 114-130) with its sweeps on the device.
+void run_generator(const Input& in) {
+    std::printf("Number of Processors: \t\t%i\n", 1);  // the lattice is generated whole on one GPU
+    std::printf("Number of Active Processors: \t%i\n\n", 1);
+    mkdir(in.output_dir.c_str(), 0755);  // OutputObs::setOutputDir creates both (outputobs.cpp:19-22)
+    mkdir((in.output_dir + "/flow").c_str(), 0755);
+    const std::string obs_path = in.output_dir + "/observables.dat";
+    FILE* o = std::fopen(obs_path.c_str(), "w+");  // OutputObs::initialize (outputobs.cpp:29-39)
+    if (!o) die("cannot write " + obs_path);
+    std::fprintf(o, "Step\t");
+    if (in.measure) std::fprintf(o, "%s\t%s\t%s\t", "Plaq.", "Topc.", "Energ.");
+    std::fprintf(o, "\n");
+    std::fclose(o);
+    const std::string full_path = in.output_dir + "/observables.full.dat";
+    FILE* p = std::fopen(full_path.c_str(), "w+");
+    if (!p) die("cannot write " + full_path);
+    std::fprintf(p, "step\tconf\tplaq\ttopc\tenergy\tacceptance\n");
+
+    int st = 0;
+    ymflow_ctx* ctx = ymflow_create(in.size, in.precision, in.device, &st);
+    if (!ctx) die(std::string("ymflow_create: ") + ymflow_last_error(nullptr));
+    const double tries_per_sweep = double(in.hits) * 4.0 * double(in.size[0]) * in.size[1] * in.size[2] * in.size[3];
+    double accepted = 0.0, tries = 0.0;  // cumulative, as m_accepted / m_updates
+    auto sweeps = [&](int start, int n) {
+        double frac = 0.0;
+        check(ymflow_generate_metropolis(ctx, start, in.beta, in.su3eps, n, in.hits, in.seed, &frac), ctx,
+              "metropolis");
+        accepted += std::round(frac * n * tries_per_sweep);
+        tries += n * tries_per_sweep;
+    };
+    // OutputTerm::printThermStep / printGenStep (outputterm.cpp:29-51)
+    auto report = [&](const char* head, int num) {
+        ymflow_obs ob{};
+        std::printf(head, num);
+        if (in.measure) {
+            check(ymflow_observables(ctx, &ob), ctx, "observables");
+            std::printf("\t%s\t = %lf \n", "Plaq.", ob.plaq);
+            std::printf("\t%s\t = %lf \n", "Topc.", ob.topc);
+            std::printf("\t%s\t = %lf \n", "Energ.", ob.energy);
+        }
+        std::printf("\tAccept. Ratio = %lf\n", accepted / tries);
+        return ob;
+    };
+
+    sweeps(in.hot ? YMFLOW_FIELD_HOT : YMFLOW_FIELD_COLD, 0);  // initialize (gaugefieldfactory.cpp:62-73)
+    const int k = in.corr_steps;
+    for (int step = k; step <= in.therm_steps; step += k) {  // thermalize (:97-108)
+        sweeps(YMFLOW_FIELD_CURRENT, k);
+        report("Thermalization Step %4i\n", step);
+    }
+    if (in.therm_steps % k) sweeps(YMFLOW_FIELD_CURRENT, in.therm_steps % k);
+    // sampleConf (:114-130).  Sweeps after the last saved configuration change
+    // no output and are not run.
+    int conf_num = 0;
+    for (int step = k; step <= in.mc_steps; step += k) {
+        sweeps(YMFLOW_FIELD_CURRENT, k);
+        const ymflow_obs ob = report("Configuration Number %4i\n", conf_num);
+        if (FILE* w = std::fopen(obs_path.c_str(), "a")) {  // OutputObs::writeObs (outputobs.cpp:47-57)
+            std::fprintf(w, "%i\t", step);
+            if (in.measure) std::fprintf(w, "%lf\t%lf\t%lf\t", ob.plaq, ob.topc, ob.energy);
+            std::fprintf(w, "\n");
+            std::fclose(w);
+        }
+        std::fprintf(p, "%d\t%d\t%.17g\t%.17g\t%.17g\t%.17g\n", step, conf_num, ob.plaq, ob.topc, ob.energy,
+                     accepted / tries);
+        std::fflush(p);
+        write_conf(ctx, in, conf_num);
+        conf_num++;
+    }
+    std::fclose(p);
+    ymflow_destroy(ctx);
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -188,6 +347,12 @@ int main(int argc, char** argv) {
 
     std::printf("Total Lattice Size: %2i %2i %2i %2i\n", in.size[0], in.size[1], in.size[2], in.size[3]);
     std::printf("Sublattice Size:    %2i %2i %2i %2i\n\n", in.sub[0], in.sub[1], in.sub[2], in.sub[3]);
+    if (in.generate) {
+        run_generator(in);
+        const std::chrono::duration<double> el = std::chrono::system_clock::now() - start;
+        std::printf("Total time taken: %.2fs\n", el.count());
+        return 0;
+    }
     // time slabs when SubLatticeSize splits only t
     int nslabs = 1;
     if (in.sub[0] == in.size[0] && in.sub[1] == in.size[1] && in.sub[2] == in.size[2] && in.sub[3] < in.size[3] &&

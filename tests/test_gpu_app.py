@@ -113,3 +113,84 @@ def test_flow_app_mixed_precision_rows(tmp_path):
         va, vb = [float(x) for x in a.split()], [float(x) for x in b.split()]
         assert va[0] == vb[0]
         assert abs(va[1] - vb[1]) < 2e-6 and abs(va[3] - vb[3]) < 1e-6 * abs(vb[3]) + 2e-6
+
+
+def _pgfg(tmp_path, params, extra=None):
+    import json
+
+    cfg = {"App": {"type": "PGFG", "params": params},
+           "LatticeSize": {"x": 4, "y": 4, "z": 4, "t": 4}, "SubLatticeSize": {"x": 4, "y": 4, "z": 4, "t": 4},
+           "Action": {"type": "puregauge", "params": {"beta": 6.0}}, "Observables": ["superobs"],
+           "OutputDir": str(tmp_path / "out")}
+    cfg.update(extra or {})
+    (tmp_path / "gen.json").write_text(json.dumps(cfg))
+    return subprocess.run([str(APP), str(tmp_path / "gen.json")], capture_output=True, text=True, check=True)
+
+
+@pytest.mark.parametrize("params,extra,therm_reports,saved_after", [
+    # NConf 3 of 6 MC steps: a configuration every 2 sweeps, after 4 thermalisation sweeps
+    ({"startType": "Cold", "MCSteps": 6, "thermSteps": 4, "SU3eps": 0.24, "NConf": 3}, {},
+     [2, 4], [6, 8, 10]),
+    # NCorr 4 of 6: NConf = 1, so 6 sweeps between configurations (the reference's integer arithmetic);
+    # 3 thermalisation sweeps, no report; FP32 links, seed 5, big-endian files
+    ({"startType": "Hot", "MCSteps": 6, "thermSteps": 3, "SU3eps": 0.3, "NCorr": 4},
+     {"Precision": "fp32_18", "Seed": 5, "Endian": "big"}, [], [9]),
+])
+def test_generator_app_writes_the_seeded_chain(tmp_path, params, extra, therm_reports, saved_after):
+    """The PGFG application: its thermalisation and sampling loops over the
+    device Metropolis, each saved confNNNN.bin equal (bit for bit) to the same
+    seeded chain run as one ymflow_generate_metropolis call, and its
+    observables those of the saved field."""
+    import numpy as np
+
+    from latticeyangmills_b200 import GluonField, read_conf
+
+    res = _pgfg(tmp_path, params, extra)
+    out = tmp_path / "out"
+    assert res.stdout.count("Thermalization Step") == len(therm_reports)
+    for s in therm_reports:
+        assert "Thermalization Step %4i\n" % s in res.stdout
+    assert res.stdout.count("Configuration Number") == len(saved_after)
+    assert res.stdout.count("\tAccept. Ratio = ") == len(therm_reports) + len(saved_after)
+    rows = (out / "observables.dat").read_text().splitlines()
+    assert rows[0] == "Step\tPlaq.\tTopc.\tEnerg.\t"
+    k = saved_after[0] - params["thermSteps"]
+    assert [r.split("\t")[0] for r in rows[1:]] == [str(k * (i + 1)) for i in range(len(saved_after))]
+    full = np.loadtxt(out / "observables.full.dat", skiprows=1, ndmin=2)
+    assert sorted(p.name for p in out.glob("conf*.bin")) == ["conf%04d.bin" % i for i in range(len(saved_after))]
+    n = (4, 4, 4, 4)
+    prec = extra.get("Precision", "fp64")
+    big = extra.get("Endian") == "big"
+    with GluonField(n, prec) as f:
+        for i, total in enumerate(saved_after):
+            acc = f.generate_metropolis(6.0, params["SU3eps"], total, 30, extra.get("Seed", 1),
+                                        params["startType"].lower())
+            want = f.download()
+            got = read_conf(out / ("conf%04d.bin" % i), n, big_endian=big)
+            assert np.array_equal(got, want), i
+            o = f.observables()
+            assert full[i, 2] == o.plaq and full[i, 3] == o.topc and full[i, 4] == o.energy
+            assert abs(full[i, 5] - acc) <= 1e-14 * acc
+            assert rows[i + 1].split("\t")[1] == "%f" % o.plaq
+            assert "Configuration Number %4i\n\tPlaq.\t = %f \n" % (i, o.plaq) in res.stdout
+
+
+def test_generated_configurations_flow_through_the_flow_app(tmp_path):
+    """Generator then flow, both drop-in applications: the FLOW app reads the
+    PGFG app's confNNNN.bin files and its first row is their plaquette."""
+    import json
+
+    import numpy as np
+
+    _pgfg(tmp_path, {"startType": "Cold", "MCSteps": 4, "thermSteps": 2, "SU3eps": 0.24, "NConf": 2})
+    full = np.loadtxt(tmp_path / "out" / "observables.full.dat", skiprows=1, ndmin=2)
+    cfg = json.loads((GOLDEN / "app_flow" / "input.json").read_text()
+                     .replace("@IN@", str(tmp_path / "out")).replace("@OUT@", str(tmp_path / "flowed")))
+    (tmp_path / "flow.json").write_text(json.dumps(cfg))
+    subprocess.run([str(APP), str(tmp_path / "flow.json")], capture_output=True, text=True, check=True)
+    for i in range(2):
+        rows = (tmp_path / "flowed" / "flow" / ("conf%04d.full.dat" % i)).read_text().splitlines()
+        first = [float(x) for x in rows[1].split("\t")]
+        assert first[2] == full[i, 2]
+        last = [float(x) for x in rows[-1].split("\t")]
+        assert last[2] > first[2]  # the flow smooths: the plaquette rises

@@ -64,9 +64,20 @@ def _app_input(tmp_path, extra):
     return tmp_path / "run.json"
 
 
+PGFG_OK = {"startType": "Cold", "MCSteps": 6, "thermSteps": 4, "SU3eps": 0.24, "NConf": 3}
+
+
 @pytest.mark.parametrize("bad,msg", [
     ({"App": {"type": "FLOW", "params": {"epsilon": 0.01}}}, "wrong \"FLOW\" app specification"),
-    ({"App": {"type": "PGFG", "params": {}}}, "only \"FLOW\""),
+    ({"App": {"type": "PGFG", "params": {}}}, "wrong \"PGFG\" app specification"),
+    ({"App": {"type": "PGFG", "params": dict(PGFG_OK, NCorr=2)}}, "wrong \"PGFG\" app specification"),
+    ({"App": {"type": "PGFG", "params": dict(PGFG_OK, startType="Warm")}}, "startType must be"),
+    ({"App": {"type": "PGFG", "params": dict(PGFG_OK, NConf=7)}}, "need 1 <= NConf <= MCSteps"),
+    ({"App": {"type": "PGFG", "params": {k: v for k, v in dict(PGFG_OK, NCorr=0).items() if k != "NConf"}}},
+     "NCorr must be >= 1"),
+    ({"App": {"type": "PGFG", "params": dict(PGFG_OK, SU3eps=1.5)}}, "SU3eps must lie in (0, 1)"),
+    ({"App": {"type": "PGFG", "params": PGFG_OK}, "MetropolisHits": 0}, "MetropolisHits must be >= 1"),
+    ({"App": {"type": "GFR", "params": {}}}, "\"FLOW\" and \"PGFG\" are provided"),
     ({"Observables": ["wilsonloop"]}, "unknown Observable"),
     ({"LatticeSize": {"x": 4, "y": 4, "z": 4}}, "wrong LatticeSize specification"),
     ({"Precision": "fp16"}, "unknown Precision"),
