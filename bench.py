@@ -1,8 +1,11 @@
 """Benchmark: Wilson-flow link-updates/s at 32^4, mixed (FP32 links, FP64 reductions)
 vs FP64, on B200.
 
-One "step" is one Luscher RK3 flow step (three fused stage kernels) over a whole
-32^4 configuration: 4 * 32^4 = 4,194,304 link-updates.  Inputs are seeded
+One "step" is one Luscher RK3 flow step over a whole 32^4 configuration:
+4 * 32^4 = 4,194,304 link-updates.  Per stage the mixed forms run two kernels
+(the plaquette field, then the stage built on it); FP64 runs one fused kernel.
+The default precision is the 12-real FP32 form, the fastest that holds the
+1e-6 accuracy target.  Inputs are seeded
 synthetic fields U = e^{i a H} (a = 0.35, H Gaussian traceless Hermitian per
 link), generated on the device; 32^4 links plus the generator field are larger
 than the 126 MB L2 (no flush needed).
@@ -24,8 +27,10 @@ the single slab exchanges with itself, which prices the exchange on one GPU.
   python bench.py --profile [--profile-kernel obs] --precision P   # only the timed kernels, for ncu
 
 The JSON line carries, besides the contract's keys: `roofline` (HBM, the
-stage kernel's algorithmic bytes over its event-timed launches), `alu_roofline`
-(the same launches against the measured FP32 or FP64 FMA peak),
+stage kernel's algorithmic bytes over its event-timed launches; `field_kernel`
+the same for the plaquette-field kernel of the two-kernel stage),
+`alu_roofline` (the reference algorithm's flops over the step's kernel time,
+against the measured FP32 or FP64 FMA peak),
 `accuracy_vs_fp64` (t^2 E and Q at t = 4), `ensemble` (64 configurations of
 four sizes) and `cpu_baseline` (the reference's own code on one host core).
 """
@@ -64,6 +69,17 @@ def bytes_per_link_update(prec: str) -> int:
     return 6 * LINK_BYTES[prec] + 4 * FORCE_BYTES[prec]
 
 
+def split_bytes_per_link(prec: str):
+    """Compulsory HBM bytes per link of one launch of each kernel of the
+    two-kernel stage, averaged over the three stages: the plaquette-field
+    kernel reads the link (s_U) and writes the site's six plane generators
+    (6 s_Z per site = 1.5 s_Z per link); the stage kernel reads the link and
+    the plane generators, writes the link, and moves the RK generator (4 s_Z
+    over three stages)."""
+    su, sz = LINK_BYTES[prec], FORCE_BYTES[prec]
+    return su + 1.5 * sz, 2 * su + 1.5 * sz + 4 * sz / 3.0
+
+
 # Algorithmic flops of one link through one RK3 stage, as the reference's
 # algorithm counts them: 12 staple products + U Omega + Q^2 + e^{iQ} U, 198 flops
 # per 3x3 complex product, plus about 300 scalar flops (projection, RK combine,
@@ -79,12 +95,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(prec: str, dims, alg_bytes_avg: float):
-    """DRAM bytes of an average stage launch from the committed ncu summary
-    (profiles/), or None.  The summary holds one captured launch (stage 1) with
-    its own algorithmic bytes; its traffic/algorithmic ratio is applied to the
-    average launch of the three stages."""
-    name = "rk_stage_%s_%s.md" % ("x".join(str(d) for d in dims), prec)
+def profiled_traffic(prec: str, dims, alg_bytes_avg: float, kernel: str = "rk_stage"):
+    """DRAM bytes of an average launch of `kernel` from the committed ncu
+    summary (profiles/<kernel>_<dims>_<prec>.md), or None.  The summary holds
+    one captured launch with its own algorithmic bytes; its
+    traffic/algorithmic ratio is applied to the average launch."""
+    name = "%s_%s_%s.md" % (kernel, "x".join(str(d) for d in dims), prec)
     p = ROOT / "profiles" / name
     if not p.exists():
         return None
@@ -429,8 +445,10 @@ def our_arm(args, dist: Dist):
             print(json.dumps({"profile": True, "precision": prec, "lattice": list(DIMS),
                               "ms_per_step": elapsed_ms / args.steps}))
         return
-    # stage-kernel durations, measured with events around every launch of a second timed pass
-    _, kernel_ms = f.time_steps(EPS, args.steps, kernels=True)
+    # kernel durations, measured with events around every launch of a second timed pass
+    split = f.get_option(N.OPT_STAGE_FORM) == 1
+    _, field_ms, stage_ms = f.time_kernels(EPS, args.steps)
+    kernel_ms = field_ms + stage_ms
     clocks.stop()
     t_max = dist.max(elapsed_ms / 1e3)
     value = dist.world * links * args.steps / t_max
@@ -446,16 +464,32 @@ def our_arm(args, dist: Dist):
         fp64_value = dist.world * links * args.steps / dist.max(ms64 / 1e3)
         g.close()
 
-    # roofline of the dominant kernel (the fused RK stage)
+    # roofline of the dominant kernel: the stage kernel (fused, or the second
+    # kernel of the two-kernel stage); the plaquette-field kernel beside it
     peak, peak_kind = measured_peaks()
-    bpl = bytes_per_link_update(prec) * links / 3.0  # algorithmic bytes per stage launch
-    avg_launch_s = kernel_ms / 1e3 / (3 * args.steps)
+    field_roof = None
+    if split:
+        field_b, stage_b = split_bytes_per_link(prec)
+        bpl = stage_b * links
+        kname = "rk_split_stage_kernel (RK3 stage from the plaquette field)"
+        field_s = field_ms / 1e3 / (3 * args.steps)
+        field_ach = field_b * links / field_s / 1e9
+        field_tr = profiled_traffic(prec, DIMS, field_b * links, "plaq_field")
+        field_roof = {"kernel": "plaq_field_kernel (six plane generators per site)", "bound": "hbm",
+                      "achieved": field_ach, "peak": peak, "unit": "GB/s", "frac": field_ach / peak,
+                      "traffic": field_tr, "algorithmic_bytes_per_launch": field_b * links,
+                      "avg_launch_ms": field_s * 1e3, "share_of_kernel_time": field_ms / kernel_ms}
+    else:
+        bpl = bytes_per_link_update(prec) * links / 3.0  # algorithmic bytes per stage launch
+        kname = "rk_stage_kernel (fused RK3 stage)"
+    avg_launch_s = stage_ms / 1e3 / (3 * args.steps)
     achieved = bpl / avg_launch_s / 1e9
-    traffic = profiled_traffic(prec, DIMS, bpl)
-    # arithmetic roofline: the same launches against the measured CUDA-core FMA peak
+    traffic = profiled_traffic(prec, DIMS, bpl, "rk_split_stage" if split else "rk_stage")
+    # arithmetic roofline: the reference algorithm's flops over the step's kernel
+    # time, against the measured CUDA-core FMA peak
     fma_tf = ctypes.c_double(0.0)
     N.check(N.load().ymflow_fma_peak(dev, N.FP64 if prec == "fp64" else N.FP32_18, ctypes.byref(fma_tf)))
-    alu_achieved = links * FLOPS_PER_LINK_STAGE / avg_launch_s / 1e12
+    alu_achieved = links * FLOPS_PER_LINK_STAGE / (kernel_ms / 1e3 / (3 * args.steps)) / 1e12
 
     # accuracy of the mixed form against FP64 at t = 4 (400 steps), same seeded field
     accuracy = None
@@ -507,7 +541,7 @@ def our_arm(args, dist: Dist):
     f.close()
 
     if dist.rank == 0:
-        launches = 3 * args.steps
+        launches = 3 * args.steps * (2 if split else 1)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
@@ -522,9 +556,10 @@ def our_arm(args, dist: Dist):
                        "mixed_over_fp64": (value / fp64_value) if fp64_value else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "rk_stage_kernel (fused RK3 stage)",
+                         "kernel": kname,
                          "algorithmic_bytes_per_launch": bpl,
-                         "avg_launch_ms": avg_launch_s * 1e3},
+                         "avg_launch_ms": avg_launch_s * 1e3,
+                         "field_kernel": field_roof},
             "alu_roofline": {"bound": "fp64 fma" if prec == "fp64" else "fp32 fma", "achieved": alu_achieved,
                              "peak": fma_tf.value, "unit": "TFLOP/s", "frac": alu_achieved / fma_tf.value,
                              "peak_kind": "measured (ymflow_fma_peak, 8 independent FMA chains per thread)",
@@ -614,7 +649,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32_18", choices=["fp64", "fp32_18", "fp32_12"])
+    ap.add_argument("--precision", default="fp32_12", choices=["fp64", "fp32_18", "fp32_12"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--skip-ensemble", action="store_true")

@@ -192,15 +192,27 @@ YMFLOW_API int ymflow_set_time(ymflow_ctx* ctx, int64_t step, double t);
  * duration of the stage kernels alone, timed with events around each launch. */
 YMFLOW_API int ymflow_time_steps(ymflow_ctx* ctx, double eps, int nsteps, float* elapsed_ms, float* kernel_ms);
 
+/* The same with the kernels of the two-kernel stage (YMFLOW_OPT_STAGE_FORM 1)
+ * timed apart: field_ms (optional) receives the summed duration of the
+ * plaquette-field kernels (0 for the fused form), stage_ms (optional) that of
+ * the stage kernels, each from events around every launch. */
+YMFLOW_API int ymflow_time_kernels(ymflow_ctx* ctx, double eps, int nsteps, float* elapsed_ms, float* field_ms,
+                                   float* stage_ms);
+
 /* Tuning knobs.  key YMFLOW_OPT_BLOCK: threads per block of the stage kernel
  * (128: four warps, one per direction, per 32 sites); YMFLOW_OPT_OBS_BLOCK:
  * threads per block of the observables kernel (192: six warps, one per
  * plane, per 32 sites; read-only in effect, other values are rejected);
  * YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a captured CUDA graph
- * (default), 0 = plain launches. */
+ * (default), 0 = plain launches; YMFLOW_OPT_STAGE_FORM: 0 = one fused kernel
+ * per RK3 stage (the FP64 default, and the only form of slabs), 1 = two
+ * kernels per stage, the six plaquettes' generators of every site into a
+ * stored field (6 x 8 reals per site of device memory) and each link's force
+ * from them (the FP32 default for whole-lattice contexts). */
 #define YMFLOW_OPT_BLOCK 1
 #define YMFLOW_OPT_GRAPH 2
 #define YMFLOW_OPT_OBS_BLOCK 3
+#define YMFLOW_OPT_STAGE_FORM 4
 YMFLOW_API int ymflow_set_option(ymflow_ctx* ctx, int key, int64_t value);
 YMFLOW_API int ymflow_get_option(const ymflow_ctx* ctx, int key, int64_t* value);
 

@@ -21,6 +21,8 @@ struct ymflow_ctx {
     void* u[2] = {nullptr, nullptr};  // ping-pong link buffers
     int cur = 0;                      // which of u[] holds the current field
     void* z = nullptr;                // RK generator, 8 reals per link
+    void* hfield = nullptr;           // plaquette field of the two-kernel stage (stage_form 1)
+    int stage_form = 0;               // 0: fused stage kernel, 1: plaquette field + stage kernel
     double* staging = nullptr;        // .bin-layout device buffer for upload/download
     size_t staging_bytes = 0;
     double* partials = nullptr;       // observables: 3 doubles per block

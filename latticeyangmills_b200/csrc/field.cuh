@@ -303,6 +303,14 @@ struct ForceField<double> {
     __device__ __forceinline__ Herm8<double> load(int mu, int s) const {
         const double2* q = link(mu, s);
         const double2 a = q[0], b = q[32], c = q[64], d = q[96];
+        return unpack(a, b, c, d);
+    }
+    // the same through the read-only data path (fields no thread of the kernel writes)
+    __device__ __forceinline__ Herm8<double> load_ro(int mu, int s) const {
+        const double2* q = link(mu, s);
+        return unpack(__ldg(q), __ldg(q + 32), __ldg(q + 64), __ldg(q + 96));
+    }
+    __device__ __forceinline__ static Herm8<double> unpack(double2 a, double2 b, double2 c, double2 d) {
         Herm8<double> z;
         z.d0 = a.x;
         z.d1 = a.y;
@@ -330,6 +338,14 @@ struct ForceField<float> {
     __device__ __forceinline__ Herm8<float> load(int mu, int s) const {
         const float4* q = link(mu, s);
         const float4 a = q[0], b = q[32];
+        return unpack(a, b);
+    }
+    // the same through the read-only data path (fields no thread of the kernel writes)
+    __device__ __forceinline__ Herm8<float> load_ro(int mu, int s) const {
+        const float4* q = link(mu, s);
+        return unpack(__ldg(q), __ldg(q + 32));
+    }
+    __device__ __forceinline__ static Herm8<float> unpack(float4 a, float4 b) {
         Herm8<float> z;
         z.d0 = a.x;
         z.d1 = a.y;

@@ -20,16 +20,6 @@ __device__ __forceinline__ void link_of_thread(const Geo& g, int& s, int& mu) {
     s = g.site0 + b * 32 + (threadIdx.x & 31);  // 128 threads: one 32-site group per block
 }
 
-// Resident 128-thread blocks per SM the stage kernel is compiled for (caps its
-// registers), swept at 32^4 on B200: FP64 is fastest at 4 blocks (128
-// registers), the FP32 18-real form at 6 (80 registers, 24 warps; 1.21 against
-// 1.24-1.37 ms per step at 5) and the 12-real form at 5 (96 registers; its row
-// rebuild spills heavily at 80).
-template <class F>
-struct StageMinBlocks {
-    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : (F::kElems == 9 ? 6 : 5);
-};
-
 template <class F, int STAGE>
 __global__ void __launch_bounds__(128, StageMinBlocks<F>::value)
     rk_stage_kernel(F in, F out, ForceField<typename F::Real> zf, Geo g, typename F::Real eps) {

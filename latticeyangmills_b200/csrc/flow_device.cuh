@@ -20,6 +20,16 @@
 
 namespace ym {
 
+// Resident 128-thread blocks per SM the stage kernel is compiled for (caps its
+// registers), swept at 32^4 on B200: FP64 is fastest at 4 blocks (128
+// registers), the FP32 18-real form at 6 (80 registers, 24 warps; 1.21 against
+// 1.24-1.37 ms per step at 5) and the 12-real form at 5 (96 registers; its row
+// rebuild spills heavily at 80).
+template <class F>
+struct StageMinBlocks {
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : (F::kElems == 9 ? 6 : 5);
+};
+
 // D_mu(x) = (i/2)[U Omega - (U Omega)^+]_traceless for one link; also returns U_mu(x).
 // Each staple is a product of three SU(3) links; of U Omega only the entries
 // the traceless anti-Hermitian part needs are computed.  mu is warp-uniform and the nu loop is kept rolled: one copy of
@@ -106,15 +116,15 @@ struct HaloTargets {
     int lower_t;
 };
 
-template <class F, int STAGE, bool HALO>
-__device__ __forceinline__ void rk_link_update_to(const F& in, const F& out, const ForceField<typename F::Real>& zf,
-                                                  const Geo& g, typename F::Real eps, int s, int mu,
-                                                  const HaloTargets<F>& h) {
+// The rest of a link's stage once its generator dz = D_mu(x) is known: the RK
+// combination with the stored generator, e^{i eps_s Z} and the new link
+// e^{i eps_s Z} U stored into `out` (returned for the halo stores).
+template <class F, int STAGE>
+__device__ __forceinline__ Rows2<typename F::Real> rk_finish(const F& out, const ForceField<typename F::Real>& zf,
+                                                            typename F::Real eps, int s, int mu,
+                                                            const Herm8<typename F::Real>& dz,
+                                                            const M3<typename F::Real>& u) {
     using R = typename F::Real;
-    int c[4];
-    g.coords(s, c);
-    M3<R> u;
-    const Herm8<R> dz = link_force(in, g, s, c, mu, u);
     Herm8<R> z;
     if (STAGE == 0) {
         z = dz;
@@ -130,6 +140,19 @@ __device__ __forceinline__ void rk_link_update_to(const F& in, const F& out, con
     exp_iq_rows2(q, e);
     mmul_rows2<false, false>(e, u, un);  // e^{iQ} U is in SU(3): two rows suffice
     out.store_rows2(mu, s, un);
+    return un;
+}
+
+template <class F, int STAGE, bool HALO>
+__device__ __forceinline__ void rk_link_update_to(const F& in, const F& out, const ForceField<typename F::Real>& zf,
+                                                  const Geo& g, typename F::Real eps, int s, int mu,
+                                                  const HaloTargets<F>& h) {
+    using R = typename F::Real;
+    int c[4];
+    g.coords(s, c);
+    M3<R> u;
+    const Herm8<R> dz = link_force(in, g, s, c, mu, u);
+    const Rows2<R> un = rk_finish<F, STAGE>(out, zf, eps, s, mu, dz, u);
     if constexpr (HALO) {
         if (c[3] == 1) h.lower.store_rows2(mu, h.lower_t * h.slice_sites + (s - h.slice_sites), un);
         if (c[3] == h.nt) h.upper.store_rows2(mu, s - h.nt * h.slice_sites, un);

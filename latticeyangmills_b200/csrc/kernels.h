@@ -18,6 +18,8 @@ inline size_t force_bytes(int prec) { return prec == kFP64 ? 64 : 32; }
 // device bytes of a link field / a generator field (volume padded to whole warp groups)
 inline size_t link_field_bytes(int prec, int64_t V) { return size_t(4 * padded_sites(V)) * link_bytes(prec); }
 inline size_t force_field_bytes(int prec, int64_t V) { return size_t(4 * padded_sites(V)) * force_bytes(prec); }
+// device bytes of a plaquette field: the six H_p of every site, generator-sized
+inline size_t plane_field_bytes(int prec, int64_t V) { return size_t(6 * padded_sites(V)) * force_bytes(prec); }
 // whether field.cuh's 32-bit offsets (16-byte units) reach every link of V sites
 inline bool volume_addressable(int prec, int64_t V) { return link_field_bytes(prec, V) / 16 < (size_t(1) << 32); }
 
@@ -25,6 +27,13 @@ inline bool volume_addressable(int prec, int64_t V) { return link_field_bytes(pr
 // with the stored generator, e^{i eps_stage Z} and the link update uin -> uout.
 cudaError_t launch_rk_stage(int prec, int stage, const void* uin, void* uout, void* z, const Geo& g, double eps,
                             int block, cudaStream_t st);
+
+// The same stage as two kernels (flow_split.cu): the six plaquettes' generators
+// of every site of u into h (plane_field_bytes), then the stage with each
+// link's force built from h (h must hold uin's plaquette field).
+cudaError_t launch_plaq_field(int prec, const void* u, void* h, const Geo& g, cudaStream_t st);
+cudaError_t launch_rk_split_stage(int prec, int stage, const void* uin, void* uout, void* z, const void* h,
+                                  const Geo& g, double eps, cudaStream_t st);
 
 // The same stage for a time slab (g.site0 = sites per slice, interior slices
 // [1, nt]): each new link of local slice 1 is also stored into the lower slab's

@@ -284,6 +284,93 @@ __device__ __forceinline__ Herm8<R> force_from_u_omega(const M3<R>& u, const M3<
     return z;
 }
 
+// The generator (i/2)[X - X^+]_traceless of X = B C^+ without forming X: the
+// six off-diagonal entries and the imaginary diagonal of B C^+.
+template <class R>
+__device__ __forceinline__ Herm8<R> force_from_b_cdag(const M3<R>& b, const M3<R>& c) {
+    auto entry = [&](int i, int j) {  // (B C^+)_ij = sum_k b_ik conj(c_jk)
+        R re = R(0), im = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            re = fma(b.e[i][k].re, c.e[j][k].re, re);
+            re = fma(b.e[i][k].im, c.e[j][k].im, re);
+            im = fma(b.e[i][k].im, c.e[j][k].re, im);
+            im = fma(-b.e[i][k].re, c.e[j][k].im, im);
+        }
+        return cx(re, im);
+    };
+    auto diag_im = [&](int i) {
+        R im = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            im = fma(b.e[i][k].im, c.e[i][k].re, im);
+            im = fma(-b.e[i][k].re, c.e[i][k].im, im);
+        }
+        return im;
+    };
+    Herm8<R> z;
+    const R i0 = diag_im(0), i1 = diag_im(1), i2 = diag_im(2);
+    const R mean = (i0 + i1 + i2) * R(1.0 / 3.0);
+    z.d0 = mean - i0;
+    z.d1 = mean - i1;
+    const Cx<R> x01 = entry(0, 1), x10 = entry(1, 0);
+    const Cx<R> x02 = entry(0, 2), x20 = entry(2, 0);
+    const Cx<R> x12 = entry(1, 2), x21 = entry(2, 1);
+    z.z01 = cx(R(-0.5) * (x01.im + x10.im), R(0.5) * (x01.re - x10.re));
+    z.z02 = cx(R(-0.5) * (x02.im + x20.im), R(0.5) * (x02.re - x20.re));
+    z.z12 = cx(R(-0.5) * (x12.im + x21.im), R(0.5) * (x12.re - x21.re));
+    return z;
+}
+
+// v^+ h v for a Hermitian traceless h: Hermitian and traceless again, so only
+// its diagonal d0, d1 and upper triangle are formed.  W = h v uses h's real
+// diagonal (h22 = -d0 - d1) and conjugate lower triangle.
+template <class R>
+__device__ __forceinline__ Herm8<R> herm_conj_by(const M3<R>& v, const Herm8<R>& h) {
+    const R d2 = -(h.d0 + h.d1);
+    M3<R> w;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const Cx<R> a = v.e[0][j], b = v.e[1][j], c = v.e[2][j];
+        // row 0: d0 a + z01 b + z02 c
+        w.e[0][j].re = fma(h.d0, a.re, fma(h.z01.re, b.re, fma(-h.z01.im, b.im, fma(h.z02.re, c.re, -h.z02.im * c.im))));
+        w.e[0][j].im = fma(h.d0, a.im, fma(h.z01.re, b.im, fma(h.z01.im, b.re, fma(h.z02.re, c.im, h.z02.im * c.re))));
+        // row 1: conj(z01) a + d1 b + z12 c
+        w.e[1][j].re = fma(h.z01.re, a.re, fma(h.z01.im, a.im, fma(h.d1, b.re, fma(h.z12.re, c.re, -h.z12.im * c.im))));
+        w.e[1][j].im = fma(h.z01.re, a.im, fma(-h.z01.im, a.re, fma(h.d1, b.im, fma(h.z12.re, c.im, h.z12.im * c.re))));
+        // row 2: conj(z02) a + conj(z12) b + d2 c
+        w.e[2][j].re = fma(h.z02.re, a.re, fma(h.z02.im, a.im, fma(h.z12.re, b.re, fma(h.z12.im, b.im, d2 * c.re))));
+        w.e[2][j].im = fma(h.z02.re, a.im, fma(-h.z02.im, a.re, fma(h.z12.re, b.im, fma(-h.z12.im, b.re, d2 * c.im))));
+    }
+    auto entry = [&](int i, int j) {  // (v^+ w)_ij = sum_k conj(v_ki) w_kj
+        R re = R(0), im = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            re = fma(v.e[k][i].re, w.e[k][j].re, re);
+            re = fma(v.e[k][i].im, w.e[k][j].im, re);
+            im = fma(v.e[k][i].re, w.e[k][j].im, im);
+            im = fma(-v.e[k][i].im, w.e[k][j].re, im);
+        }
+        return cx(re, im);
+    };
+    auto diag_re = [&](int i) {
+        R re = R(0);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            re = fma(v.e[k][i].re, w.e[k][i].re, re);
+            re = fma(v.e[k][i].im, w.e[k][i].im, re);
+        }
+        return re;
+    };
+    Herm8<R> r;
+    r.d0 = diag_re(0);
+    r.d1 = diag_re(1);
+    r.z01 = entry(0, 1);
+    r.z02 = entry(0, 2);
+    r.z12 = entry(1, 2);
+    return r;
+}
+
 template <class R>
 __device__ __forceinline__ Herm8<R> h8_axpby(R a, const Herm8<R>& x, R b, const Herm8<R>& y) {
     Herm8<R> r;

@@ -108,17 +108,29 @@ void drop_graphs(ymflow_ctx* c) {
     }
 }
 
-// The three stage launches of one RK3 step starting from u[from].
+// The launches of one RK3 step starting from u[from]: per stage the fused
+// stage kernel, or the plaquette-field kernel and the stage kernel built on it
+// (stage_form 1).  ev (optional): three events per stage, before the stage,
+// after its plaquette-field kernel (at once for the fused form) and after it.
 cudaError_t enqueue_step(ymflow_ctx* c, int from, double eps, cudaEvent_t* ev) {
     void* a = c->u[from];
     void* b = c->u[1 - from];
     const void* in[3] = {a, b, a};
     void* out[3] = {b, a, b};
     for (int s = 0; s < 3; s++) {
-        if (ev) cudaEventRecord(ev[2 * s], c->stream);
-        cudaError_t e = launch_rk_stage(c->prec, s, in[s], out[s], c->z, c->geo, eps, c->block, c->stream);
+        if (ev) cudaEventRecord(ev[3 * s], c->stream);
+        cudaError_t e = cudaSuccess;
+        if (c->stage_form == 1) {
+            e = launch_plaq_field(c->prec, in[s], c->hfield, c->geo, c->stream);
+            if (e != cudaSuccess) return e;
+            if (ev) cudaEventRecord(ev[3 * s + 1], c->stream);
+            e = launch_rk_split_stage(c->prec, s, in[s], out[s], c->z, c->hfield, c->geo, eps, c->stream);
+        } else {
+            if (ev) cudaEventRecord(ev[3 * s + 1], c->stream);
+            e = launch_rk_stage(c->prec, s, in[s], out[s], c->z, c->geo, eps, c->block, c->stream);
+        }
         if (e != cudaSuccess) return e;
-        if (ev) cudaEventRecord(ev[2 * s + 1], c->stream);
+        if (ev) cudaEventRecord(ev[3 * s + 2], c->stream);
     }
     return cudaSuccess;
 }
@@ -129,10 +141,13 @@ int run_step_slab(ymflow_ctx* c, double eps, cudaEvent_t* ev) {
     const int from = c->cur;
     const int in[3] = {from, 1 - from, from};
     for (int s = 0; s < 3; s++) {
-        if (ev) cudaEventRecord(ev[2 * s], c->stream);
+        if (ev) {
+            cudaEventRecord(ev[3 * s], c->stream);
+            cudaEventRecord(ev[3 * s + 1], c->stream);
+        }
         YM_CK(c, launch_rk_stage(c->prec, s, c->u[in[s]], c->u[1 - in[s]], c->z, c->geo, eps, c->block, c->stream),
               "stage launch");
-        if (ev) cudaEventRecord(ev[2 * s + 1], c->stream);
+        if (ev) cudaEventRecord(ev[3 * s + 2], c->stream);
         const int r = slab_exchange(c, 1 - in[s]);
         if (r != YMFLOW_OK) return r;
     }
@@ -284,6 +299,15 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[1], ub, "link buffer 1");
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->z, zb, "force buffer");
     if (r == YMFLOW_OK) r = dev_alloc(c, (void**)&c->deviation, sizeof(unsigned long long), "drift flag");
+    // FP32 forms flow with the two-kernel stage (plaquette field, then the
+    // stage): fewer multiply-adds per link for twice the stage's bytes, which
+    // the FP32 kernels have room for (0.98 against 1.17 ms per step at 32^4 for
+    // the 12-real form against the fused 18-real one).  FP64 keeps the fused
+    // kernel, the faster form at its two-row staple products.
+    if (r == YMFLOW_OK && c->prec != YMFLOW_FP64) {
+        r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, V), "plaquette field");
+        c->stage_form = 1;
+    }
     if (r == YMFLOW_OK) r = ensure_partials(c);
     if (r == YMFLOW_OK) r = ensure_meas(c, 16);
     if (r == YMFLOW_OK && (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess))
@@ -329,6 +353,13 @@ ymflow_ctx* ymflow_create_slab(const int global_dims[4], int t0, int nt, int pre
     if (!c) return nullptr;
     c->slab = true;
     c->geo.tile_groups = 0;  // the interior range starts at a halo slice: plain order
+    if (c->hfield) {  // slabs flow with the fused stage kernels (the halo stores are fused there)
+        DeviceGuard guard(device);
+        cudaFree(c->hfield);
+        c->bytes -= int64_t(plane_field_bytes(c->prec, c->geo.V));
+        c->hfield = nullptr;
+    }
+    c->stage_form = 0;
     c->t0 = t0;
     c->nt = nt;
     for (int i = 0; i < 4; i++) c->gdims[i] = global_dims[i];
@@ -346,7 +377,7 @@ void ymflow_destroy(ymflow_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     slab_release(c);
     drop_graphs(c);
-    for (void* p : {c->u[0], c->u[1], c->z, (void*)c->staging, (void*)c->partials, (void*)c->meas,
+    for (void* p : {c->u[0], c->u[1], c->z, c->hfield, (void*)c->staging, (void*)c->partials, (void*)c->meas,
                     (void*)c->deviation})
         if (p) cudaFree(p);
     if (c->meas_host) cudaFreeHost(c->meas_host);
@@ -681,13 +712,14 @@ int ymflow_set_time(ymflow_ctx* c, int64_t step, double t) {
     return YMFLOW_OK;
 }
 
-int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, float* kernel_ms) {
-    NvtxRange range("ymflow_time_steps");
-    if (!c || !elapsed_ms || nsteps < 1) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_time_steps");
+int ymflow_time_kernels(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, float* field_ms, float* stage_ms) {
+    NvtxRange range("ymflow_time_kernels");
+    if (!c || !elapsed_ms || nsteps < 1) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_time_kernels");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
     DeviceGuard guard(c->device);
     if (int r = slab_prepare(c)) return r;
-    const size_t nev = kernel_ms ? size_t(6) * nsteps : 0;
+    const bool per_kernel = field_ms || stage_ms;
+    const size_t nev = per_kernel ? size_t(9) * nsteps : 0;
     while (c->events.size() < nev) {
         cudaEvent_t e;
         YM_CK(c, cudaEventCreate(&e), "event create");
@@ -695,7 +727,7 @@ int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, 
     }
     YM_CK(c, cudaEventRecord(c->ev0, c->stream), "event record");
     for (int s = 0; s < nsteps; s++) {
-        int r = run_step(c, eps, kernel_ms ? c->events.data() + 6 * s : nullptr);
+        int r = run_step(c, eps, per_kernel ? c->events.data() + 9 * s : nullptr);
         if (r != YMFLOW_OK) return r;
         c->step++;
         c->t += eps;
@@ -703,16 +735,27 @@ int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, 
     YM_CK(c, cudaEventRecord(c->ev1, c->stream), "event record");
     YM_CK(c, cudaEventSynchronize(c->ev1), "timed steps");
     YM_CK(c, cudaEventElapsedTime(elapsed_ms, c->ev0, c->ev1), "elapsed time");
-    if (kernel_ms) {
-        double sum = 0.0;
+    if (per_kernel) {
+        double field = 0.0, stage = 0.0;
         for (int i = 0; i < 3 * nsteps; i++) {
-            float ms = 0.f;
-            YM_CK(c, cudaEventElapsedTime(&ms, c->events[2 * i], c->events[2 * i + 1]), "kernel time");
-            sum += ms;
+            float a = 0.f, b = 0.f;
+            YM_CK(c, cudaEventElapsedTime(&a, c->events[3 * i], c->events[3 * i + 1]), "kernel time");
+            YM_CK(c, cudaEventElapsedTime(&b, c->events[3 * i + 1], c->events[3 * i + 2]), "kernel time");
+            field += a;
+            stage += b;
         }
-        *kernel_ms = float(sum);
+        if (field_ms) *field_ms = float(field);
+        if (stage_ms) *stage_ms = float(stage);
     }
     return YMFLOW_OK;
+}
+
+int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, float* kernel_ms) {
+    float field = 0.f, stage = 0.f;
+    const int r = ymflow_time_kernels(c, eps, nsteps, elapsed_ms, kernel_ms ? &field : nullptr,
+                                      kernel_ms ? &stage : nullptr);
+    if (r == YMFLOW_OK && kernel_ms) *kernel_ms = field + stage;
+    return r;
 }
 
 int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
@@ -728,6 +771,21 @@ int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
         case YMFLOW_OPT_GRAPH:
             c->use_graph = value != 0;
             return YMFLOW_OK;
+        case YMFLOW_OPT_STAGE_FORM: {
+            if (value != 0 && value != 1) return fail(c, YMFLOW_ERR_ARG, "stage form is 0 (fused) or 1 (two kernels)");
+            if (value == 1 && c->slab) return fail(c, YMFLOW_ERR_STATE, "slabs flow with the fused stage kernel");
+            DeviceGuard guard(c->device);
+            if (value == 1 && !c->hfield) {
+                const int r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, c->geo.V), "plaquette field");
+                if (r != YMFLOW_OK) return r;
+            }
+            if (c->stage_form != int(value)) {
+                YM_CK(c, cudaStreamSynchronize(c->stream), "stage form switch");
+                drop_graphs(c);
+            }
+            c->stage_form = int(value);
+            return YMFLOW_OK;
+        }
         default: return fail(c, YMFLOW_ERR_ARG, "unknown option");
     }
 }
@@ -738,6 +796,7 @@ int ymflow_get_option(const ymflow_ctx* c, int key, int64_t* value) {
         case YMFLOW_OPT_BLOCK: *value = c->block; return YMFLOW_OK;
         case YMFLOW_OPT_OBS_BLOCK: *value = 192; return YMFLOW_OK;
         case YMFLOW_OPT_GRAPH: *value = c->use_graph ? 1 : 0; return YMFLOW_OK;
+        case YMFLOW_OPT_STAGE_FORM: *value = c->stage_form; return YMFLOW_OK;
         default: return YMFLOW_ERR_ARG;
     }
 }

@@ -231,6 +231,14 @@ class GluonField:
                                                ctypes.byref(km) if kernels else None))
         return el.value, (km.value if kernels else None)
 
+    def time_kernels(self, eps: float, nsteps: int):
+        """(elapsed_ms, plaquette-field kernels ms, stage kernels ms) of nsteps
+        device-timed RK3 steps, each kernel kind summed over its launches."""
+        el, fm, sm = ctypes.c_float(0), ctypes.c_float(0), ctypes.c_float(0)
+        self._check(N.load().ymflow_time_kernels(self.ctx, float(eps), int(nsteps), ctypes.byref(el),
+                                                 ctypes.byref(fm), ctypes.byref(sm)))
+        return el.value, fm.value, sm.value
+
     def set_option(self, key: int, value: int) -> None:
         self._check(N.load().ymflow_set_option(self.ctx, int(key), int(value)))
 

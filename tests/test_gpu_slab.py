@@ -11,9 +11,10 @@ N8 = (8, 4, 4, 10)  # spatial volume 128 (whole warp groups), 10 time slices
 
 
 def whole(precision, n=N8, seed=11, steps=6, every=2):
-    from latticeyangmills_b200 import GluonField
+    from latticeyangmills_b200 import GluonField, _native as N
 
     with GluonField(n, precision) as f:
+        f.set_option(N.OPT_STAGE_FORM, 0)  # slabs run the fused stage kernel: compare like with like
         f.init_links("expiah", 0.4, seed)
         U0 = f.download()
         rows = f.flow(0.02, steps, every, reunit_every=3 if precision != "fp64" else 0)
