@@ -106,6 +106,7 @@ def test_kernel_timing_splits_by_kernel():
         assert el > 0 and field > 0 and stage > 0 and field + stage <= el * 1.05
         f.set_option(N.OPT_STAGE_FORM, 0)
         el, field, stage = f.time_kernels(0.01, 4)
-        assert field < 0.05 * stage  # two back-to-back events: no kernel between them
+        # two back-to-back events (no kernel between them): a few microseconds per stage
+        assert field / (3 * 4) < 0.01
         _, km = f.time_steps(0.01, 4, kernels=True)
         assert km > 0
