@@ -28,6 +28,7 @@ struct EnsConf {
     Geo g;
     int64_t uoff;  // start of this configuration in the link pool (bytes, 16-aligned)
     int64_t zoff;  // start in the generator pool (bytes, 16-aligned)
+    int64_t hoff;  // start in the plane-generator pool of the two-kernel stage (bytes, 16-aligned)
     int blk0;      // first work item
     int nblk;      // work items (blocks of sites)
 };
@@ -116,6 +117,63 @@ static cudaError_t launch_ens_typed(int stage, void* uin, void* uout, void* z, c
     return cudaGetLastError();
 }
 
+// The two-kernel stage over the work list (FP32 ensembles): one 192-thread block
+// per 32-site item forms that item's six plane generators, then one 128-thread
+// block per item runs the stage from them.  One block per item, as the flat kernel.
+template <class F>
+__global__ void __launch_bounds__(192) ens_plaq_kernel(char* u, char* h, const EnsConf* __restrict__ confs, int nconf) {
+    const int item = blockIdx.x;
+    const EnsConf& C = confs[find_conf(confs, nconf, item)];
+    const Geo& g = C.g;
+    const int s = (item - C.blk0) * 32 + int(threadIdx.x & 31);
+    if (s >= g.V) return;
+    const F uf{u + C.uoff, g.V};
+    const ForceField<typename F::Real> hf{h + C.hoff, g.V};
+    plaq_plane(uf, hf, g, s, int(threadIdx.x >> 5));
+}
+
+template <class F, int STAGE>
+__global__ void __launch_bounds__(128, SplitMinBlocks<F>::value)
+    ens_split_kernel(char* uin, char* uout, char* z, char* h, const EnsConf* __restrict__ confs, int nconf,
+                     typename F::Real eps) {
+    using R = typename F::Real;
+    const int mu = int(threadIdx.x >> 5) & 3;
+    const int item = blockIdx.x;
+    const EnsConf& C = confs[find_conf(confs, nconf, item)];
+    const Geo& g = C.g;
+    const int s = (item - C.blk0) * 32 + int(threadIdx.x & 31);
+    if (s >= g.V) return;
+    const F in{uin + C.uoff, g.V}, out{uout + C.uoff, g.V};
+    const ForceField<R> zf{z + C.zoff, g.V}, hf{h + C.hoff, g.V};
+    split_link_update<F, STAGE>(in, out, zf, hf, g, eps, s, mu);
+}
+
+template <class F>
+static cudaError_t launch_ens_split_typed(int stage, void* uin, void* uout, void* z, void* h, const EnsConf* confs,
+                                          int nconf, int nitems, double eps, cudaStream_t st) {
+    using R = typename F::Real;
+    const R e = R(stage == 0 ? eps * 0.25 : eps);
+    char *a = (char*)uin, *b = (char*)uout, *zz = (char*)z, *hh = (char*)h;
+    ens_plaq_kernel<F><<<nitems, 192, 0, st>>>(a, hh, confs, nconf);
+    switch (stage) {
+        case 0: ens_split_kernel<F, 0><<<nitems, 128, 0, st>>>(a, b, zz, hh, confs, nconf, e); break;
+        case 1: ens_split_kernel<F, 1><<<nitems, 128, 0, st>>>(a, b, zz, hh, confs, nconf, e); break;
+        default: ens_split_kernel<F, 2><<<nitems, 128, 0, st>>>(a, b, zz, hh, confs, nconf, e); break;
+    }
+    return cudaGetLastError();
+}
+
+// Work items must be 32-site groups (block 128).
+cudaError_t launch_ens_split_stage(int prec, int stage, void* uin, void* uout, void* z, void* h, const EnsConf* confs,
+                                   int nconf, int nitems, double eps, cudaStream_t st) {
+    switch (prec) {
+        case kFP64: return launch_ens_split_typed<FieldD18>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st);
+        case kFP32_18: return launch_ens_split_typed<FieldF18>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st);
+        case kFP32_12: return launch_ens_split_typed<FieldF12>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_ens_stage(int prec, int stage, void* uin, void* uout, void* z, const EnsConf* confs, int nconf,
                              int nitems, int grid, int block, double eps, cudaStream_t st) {
     switch (prec) {
@@ -159,6 +217,8 @@ struct ymflow_ens {
     void* u[2] = {nullptr, nullptr};
     int cur = 0;
     void* z = nullptr;
+    void* h = nullptr;       // plane generators of the two-kernel stage (FP32 ensembles)
+    bool split = false;      // FP32: the two-kernel stage, one block per work item
     int64_t pool_links = 0;  // bytes per link pool
     int64_t pool_force = 0;  // bytes of the generator pool
     double* staging = nullptr;  // .bin-layout buffer sized for the largest configuration
@@ -229,8 +289,10 @@ cudaError_t enqueue_ens_step(ymflow_ens* e, int from, double eps) {
     const int ni = nitems(e);
     const int grid = e->grid > 0 ? std::min(e->grid, ni) : ni;
     for (int s = 0; s < 3; s++) {
-        cudaError_t r = launch_ens_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf, ni, grid, e->block,
-                                         eps, e->stream);
+        cudaError_t r = e->split ? launch_ens_split_stage(e->prec, s, in[s], out[s], e->z, e->h, e->confs_dev,
+                                                          e->nconf, ni, eps, e->stream)
+                                 : launch_ens_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf, ni, grid,
+                                                    e->block, eps, e->stream);
         if (r != cudaSuccess) return r;
     }
     return cudaSuccess;
@@ -365,7 +427,7 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
     e->device = device;
     e->confs.resize(nconf);
     e->loaded.assign(nconf, 0);
-    int64_t uo = 0, zo = 0;
+    int64_t uo = 0, zo = 0, ho = 0;
     for (int c = 0; c < nconf; c++) {
         const int* d = dims + 4 * c;
         int64_t V = 1;
@@ -386,8 +448,10 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
         C.g = make_geo(d);
         C.uoff = uo;
         C.zoff = zo;
+        C.hoff = ho;
         uo += int64_t(link_field_bytes(e->prec, V));
         zo += int64_t(force_field_bytes(e->prec, V));
+        ho += int64_t(plane_field_bytes(e->prec, V));
         e->max_v = std::max(e->max_v, V);
         e->signature += std::to_string(d[0]) + "x" + std::to_string(d[1]) + "x" + std::to_string(d[2]) + "x" +
                         std::to_string(d[3]) + ";";
@@ -400,6 +464,9 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
     if (r == YMFLOW_OK) r = ens_alloc(e, &e->u[0], size_t(uo), "link pool 0");
     if (r == YMFLOW_OK) r = ens_alloc(e, &e->u[1], size_t(uo), "link pool 1");
     if (r == YMFLOW_OK) r = ens_alloc(e, &e->z, size_t(zo), "generator pool");
+    // FP32 ensembles flow with the two-kernel stage, as FP32 single contexts do
+    e->split = precision != YMFLOW_FP64;
+    if (r == YMFLOW_OK && e->split) r = ens_alloc(e, &e->h, size_t(ho), "plane-generator pool");
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->confs_dev, sizeof(EnsConf) * nconf, "work list");
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->deviation, sizeof(unsigned long long), "drift flag");
     if (r == YMFLOW_OK) {
@@ -435,7 +502,7 @@ void ymflow_ensemble_destroy(ymflow_ens* e) {
     DeviceGuard guard(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
     drop_graphs(e);
-    for (void* p : {e->u[0], e->u[1], e->z, (void*)e->confs_dev, (void*)e->staging, (void*)e->partials,
+    for (void* p : {e->u[0], e->u[1], e->z, e->h, (void*)e->confs_dev, (void*)e->staging, (void*)e->partials,
                     (void*)e->meas, (void*)e->deviation})
         if (p) cudaFree(p);
     if (e->meas_host) cudaFreeHost(e->meas_host);
@@ -593,6 +660,16 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     for (int c = 0; c < e->nconf; c++)
         if (!e->loaded[c]) return efail(e, YMFLOW_ERR_STATE, "configuration not loaded");
     DeviceGuard guard(e->device);
+    if (e->split) {  // the two-kernel stage runs one block per 32-site item: nothing to tune
+        int r = set_block(e, 128);
+        if (r != YMFLOW_OK) return r;
+        e->grid = 0;
+        drop_graphs(e);
+        e->tuned = true;
+        if (block_out) *block_out = 128;
+        if (grid_out) *grid_out = 0;
+        return YMFLOW_OK;
+    }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
     float best = 1e30f;

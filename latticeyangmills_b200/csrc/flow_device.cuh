@@ -165,4 +165,78 @@ __device__ __forceinline__ void rk_link_update(const F& in, const F& out, const 
     rk_link_update_to<F, STAGE, false>(in, out, zf, g, eps, s, mu, HaloTargets<F>{});
 }
 
+// ---------------------------------------------------------------------------
+// The two-kernel stage (derivation in flow_split.cu): a field of the six plane
+// generators H_p(x) = (i/2)[P_p(x) - P_p(x)^+]_TL per site, then each link's
+//   D_mu(x) = sum_{nu != mu} s_{mu nu} [ H_p(x) - U_nu(y)^+ H_p(y) U_nu(y) ],  y = x - nu.
+// ---------------------------------------------------------------------------
+
+// plane index of directions a < b: (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) -> 0..5
+__device__ __forceinline__ int plane_index(int a, int b) { return a * (5 - a) / 2 + b - 1; }
+
+// H_p(x) of plane p at site s into hf.
+template <class F>
+__device__ __forceinline__ void plaq_plane(const F& u, const ForceField<typename F::Real>& hf, const Geo& g, int s,
+                                           int p) {
+    using R = typename F::Real;
+    const int a = p < 3 ? 0 : (p < 5 ? 1 : 2);
+    const int b = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
+    int c[4];
+    g.coords(s, c);
+    const int s_pa = g.hop_rt(s, g.coord(c, a), a, +1);
+    const int s_pb = g.hop_rt(s, g.coord(c, b), b, +1);
+    M3<R> lo, up;  // U_a(x) U_b(x+a) and U_b(x) U_a(x+b): P = lo up^+
+    {
+        const M3<R> x = u.load(a, s);
+        const M3<R> y = u.load(b, s_pa);
+        mmul<false, false>(x, y, lo);
+    }
+    {
+        const M3<R> x = u.load(b, s);
+        const M3<R> y = u.load(a, s_pb);
+        mmul<false, false>(x, y, up);
+    }
+    hf.store(p, s, force_from_b_cdag(lo, up));
+}
+
+// One link through one stage with its generator built from the plane field hf
+// (which holds the plane generators of `in`).
+template <class F, int STAGE>
+__device__ __forceinline__ void split_link_update(const F& in, const F& out, const ForceField<typename F::Real>& zf,
+                                                  const ForceField<typename F::Real>& hf, const Geo& g,
+                                                  typename F::Real eps, int s, int mu) {
+    using R = typename F::Real;
+    int c[4];
+    g.coords(s, c);
+    Herm8<R> d;
+    d.d0 = d.d1 = R(0);
+    d.z01 = d.z02 = d.z12 = cx(R(0), R(0));
+#pragma unroll 1
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == mu) continue;
+        const int p = mu < nu ? plane_index(mu, nu) : plane_index(nu, mu);
+        const R sg = mu < nu ? R(1) : R(-1);
+        const int y = g.hop_rt(s, g.coord(c, nu), nu, -1);
+        const M3<R> v = in.load(nu, y);
+        const Herm8<R> lower = herm_conj_by(v, hf.load_ro(p, y));
+        const Herm8<R> upper = hf.load_ro(p, s);
+        d.d0 = fma(sg, upper.d0 - lower.d0, d.d0);
+        d.d1 = fma(sg, upper.d1 - lower.d1, d.d1);
+        d.z01 = cx(fma(sg, upper.z01.re - lower.z01.re, d.z01.re), fma(sg, upper.z01.im - lower.z01.im, d.z01.im));
+        d.z02 = cx(fma(sg, upper.z02.re - lower.z02.re, d.z02.re), fma(sg, upper.z02.im - lower.z02.im, d.z02.im));
+        d.z12 = cx(fma(sg, upper.z12.re - lower.z12.re, d.z12.re), fma(sg, upper.z12.im - lower.z12.im, d.z12.im));
+    }
+    const M3<R> uu = in.load(mu, s);
+    rk_finish<F, STAGE>(out, zf, eps, s, mu, d, uu);
+}
+
+// Resident blocks of the two-kernel stage kernel: FP32 forms at 8 (64
+// registers, 32 warps per SM): 0.98 ms per RK3 step for the 12-real form at
+// 32^4 on B200 against 1.05 at the 76 registers of 6 blocks; FP64 at 4 (its
+// fused kernel's budget).
+template <class F>
+struct SplitMinBlocks {
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : 8;
+};
+
 }  // namespace ym
