@@ -583,7 +583,7 @@ def decomposed_run(args, dist: Dist):
 
     import numpy as np
 
-    from latticeyangmills_b200 import GluonField, nccl_unique_id, slab_partition
+    from latticeyangmills_b200 import GluonField, _native as N, nccl_unique_id, slab_partition
 
     prec = args.precision
     V = DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]
@@ -605,14 +605,21 @@ def decomposed_run(args, dist: Dist):
     dist.barrier()
     elapsed_ms, _ = f.time_steps(EPS, args.steps)
     dist.barrier()
-    _, kernel_ms = f.time_steps(EPS, args.steps, kernels=True)
+    split = f.get_option(N.OPT_STAGE_FORM) == 1
+    _, field_ms, stage_ms = f.time_kernels(EPS, args.steps)
+    kernel_ms = field_ms + stage_ms
     clocks.stop()
     t_max = dist.max(elapsed_ms / 1e3)
     value = 4 * V * args.steps / t_max
     peak, peak_kind = measured_peaks()
     links_local = 4 * DIMS[0] * DIMS[1] * DIMS[2] * nt
-    bpl = bytes_per_link_update(prec) * links_local / 3.0
-    avg_launch_s = kernel_ms / 1e3 / (3 * args.steps)
+    if split:
+        bpl = split_bytes_per_link(prec)[1] * links_local
+        kname = "rk_split_stage_kernel on rank 0's slab"
+    else:
+        bpl = bytes_per_link_update(prec) * links_local / 3.0
+        kname = "rk_stage_kernel on rank 0's slab"
+    avg_launch_s = stage_ms / 1e3 / (3 * args.steps)
     # end to end: every rank uploads its slab from pinned host memory, flows, reads the rows
     host = np.ascontiguousarray(f.download())
     t0w = time.perf_counter()
@@ -633,13 +640,14 @@ def decomposed_run(args, dist: Dist):
                        "l2": "inputs larger than L2 (links + generator > 126 MB per rank at N <= 2)"},
             "roofline": {"bound": "hbm", "achieved": bpl / avg_launch_s / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": bpl / avg_launch_s / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "rk_stage_kernel on rank 0's slab", "avg_launch_ms": avg_launch_s * 1e3},
+                         "kernel": kname, "avg_launch_ms": avg_launch_s * 1e3,
+                         "field_kernel_ms_per_launch": field_ms / (3 * args.steps) if split else None},
             "e2e": {"value": 4 * V * args.steps / t_e2e, "unit": UNIT,
                     "h2d_bytes_per_step": host.nbytes * dist.world / args.steps,
                     "d2h_bytes_per_step": 2 * 48 / args.steps,
                     "what": "per rank: upload of its slab from host memory, a K-step collective flow, rows back",
                     "t_end": float(rows[-1, 1])},
-            "gpu_launches": 3 * args.steps, "clocks": clocks.summary(), "cpu_baseline": None,
+            "gpu_launches": 3 * args.steps * (2 if split else 1), "clocks": clocks.summary(), "cpu_baseline": None,
         }))
 
 

@@ -205,10 +205,10 @@ YMFLOW_API int ymflow_time_kernels(ymflow_ctx* ctx, double eps, int nsteps, floa
  * plane, per 32 sites; read-only in effect, other values are rejected);
  * YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a captured CUDA graph
  * (default), 0 = plain launches; YMFLOW_OPT_STAGE_FORM: 0 = one fused kernel
- * per RK3 stage (the FP64 default, and the only form of slabs), 1 = two
- * kernels per stage, the six plaquettes' generators of every site into a
- * stored field (6 x 8 reals per site of device memory) and each link's force
- * from them (the FP32 default for whole-lattice contexts). */
+ * per RK3 stage (the FP64 default), 1 = two kernels per stage, the six
+ * plaquettes' generators of every site into a stored field (6 x 8 reals per
+ * site of device memory) and each link's force from them (the FP32 default).
+ * Slabs flowing together (ymflow_slab_group_flow) must share one form. */
 #define YMFLOW_OPT_BLOCK 1
 #define YMFLOW_OPT_GRAPH 2
 #define YMFLOW_OPT_OBS_BLOCK 3

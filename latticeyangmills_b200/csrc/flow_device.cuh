@@ -200,11 +200,13 @@ __device__ __forceinline__ void plaq_plane(const F& u, const ForceField<typename
 }
 
 // One link through one stage with its generator built from the plane field hf
-// (which holds the plane generators of `in`).
-template <class F, int STAGE>
-__device__ __forceinline__ void split_link_update(const F& in, const F& out, const ForceField<typename F::Real>& zf,
-                                                  const ForceField<typename F::Real>& hf, const Geo& g,
-                                                  typename F::Real eps, int s, int mu) {
+// (which holds the plane generators of `in`); HALO: a slab's boundary links
+// also go into its neighbours' halos, as in rk_link_update_to.
+template <class F, int STAGE, bool HALO>
+__device__ __forceinline__ void split_link_update_to(const F& in, const F& out,
+                                                     const ForceField<typename F::Real>& zf,
+                                                     const ForceField<typename F::Real>& hf, const Geo& g,
+                                                     typename F::Real eps, int s, int mu, const HaloTargets<F>& h) {
     using R = typename F::Real;
     int c[4];
     g.coords(s, c);
@@ -227,7 +229,18 @@ __device__ __forceinline__ void split_link_update(const F& in, const F& out, con
         d.z12 = cx(fma(sg, upper.z12.re - lower.z12.re, d.z12.re), fma(sg, upper.z12.im - lower.z12.im, d.z12.im));
     }
     const M3<R> uu = in.load(mu, s);
-    rk_finish<F, STAGE>(out, zf, eps, s, mu, d, uu);
+    const Rows2<R> un = rk_finish<F, STAGE>(out, zf, eps, s, mu, d, uu);
+    if constexpr (HALO) {
+        if (c[3] == 1) h.lower.store_rows2(mu, h.lower_t * h.slice_sites + (s - h.slice_sites), un);
+        if (c[3] == h.nt) h.upper.store_rows2(mu, s - h.nt * h.slice_sites, un);
+    }
+}
+
+template <class F, int STAGE>
+__device__ __forceinline__ void split_link_update(const F& in, const F& out, const ForceField<typename F::Real>& zf,
+                                                  const ForceField<typename F::Real>& hf, const Geo& g,
+                                                  typename F::Real eps, int s, int mu) {
+    split_link_update_to<F, STAGE, false>(in, out, zf, hf, g, eps, s, mu, HaloTargets<F>{});
 }
 
 // Resident blocks of the two-kernel stage kernel: FP32 forms at 8 (64

@@ -43,6 +43,36 @@ __global__ void __launch_bounds__(128, SplitMinBlocks<F>::value)
     split_link_update<F, STAGE>(in, out, zf, hf, g, eps, s, mu);
 }
 
+// The same for a time slab, storing its boundary links into its neighbours'
+// halos (the two-kernel form of rk_stage_halo_kernel).
+template <class F, int STAGE>
+__global__ void __launch_bounds__(128, SplitMinBlocks<F>::value)
+    rk_split_stage_halo_kernel(F in, F out, ForceField<typename F::Real> zf, ForceField<typename F::Real> hf, Geo g,
+                               typename F::Real eps, HaloTargets<F> h) {
+    const int mu = int(threadIdx.x >> 5) & 3;
+    const int s = g.site0 + int(blockIdx.x) * 32 + int(threadIdx.x & 31);
+    if (s >= g.site1) return;
+    split_link_update_to<F, STAGE, true>(in, out, zf, hf, g, eps, s, mu, h);
+}
+
+template <class F>
+static cudaError_t launch_split_halo_typed(int stage, const void* uin, void* uout, void* z, const void* hp,
+                                           const Geo& g, double eps, void* lower_out, int lower_v, int lower_t,
+                                           void* upper_out, int upper_v, cudaStream_t st) {
+    using R = typename F::Real;
+    F in{const_cast<void*>(uin), g.V}, out{uout, g.V};
+    ForceField<R> zf{z, g.V}, hf{const_cast<void*>(hp), g.V};
+    HaloTargets<F> h{F{lower_out, lower_v}, F{upper_out, upper_v}, g.site0, (g.site1 - g.site0) / g.site0, lower_t};
+    const dim3 grid(unsigned((g.site1 - g.site0 + 31) / 32));
+    const R e = R(stage == 0 ? eps * 0.25 : eps);
+    switch (stage) {
+        case 0: rk_split_stage_halo_kernel<F, 0><<<grid, 128, 0, st>>>(in, out, zf, hf, g, e, h); break;
+        case 1: rk_split_stage_halo_kernel<F, 1><<<grid, 128, 0, st>>>(in, out, zf, hf, g, e, h); break;
+        default: rk_split_stage_halo_kernel<F, 2><<<grid, 128, 0, st>>>(in, out, zf, hf, g, e, h); break;
+    }
+    return cudaGetLastError();
+}
+
 template <class F>
 static cudaError_t launch_plaq_typed(const void* u, void* h, const Geo& g, cudaStream_t st) {
     F in{const_cast<void*>(u), g.V};
@@ -72,6 +102,24 @@ cudaError_t launch_plaq_field(int prec, const void* u, void* h, const Geo& g, cu
         case kFP64: return launch_plaq_typed<FieldD18>(u, h, g, st);
         case kFP32_18: return launch_plaq_typed<FieldF18>(u, h, g, st);
         case kFP32_12: return launch_plaq_typed<FieldF12>(u, h, g, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_rk_split_stage_halo(int prec, int stage, const void* uin, void* uout, void* z, const void* h,
+                                       const Geo& g, double eps, void* lower_out, int lower_v, int lower_t,
+                                       void* upper_out, int upper_v, cudaStream_t st) {
+    if (g.site0 <= 0 || g.site0 % 32 || (g.site1 - g.site0) % g.site0) return cudaErrorInvalidValue;
+    switch (prec) {
+        case kFP64:
+            return launch_split_halo_typed<FieldD18>(stage, uin, uout, z, h, g, eps, lower_out, lower_v, lower_t,
+                                                     upper_out, upper_v, st);
+        case kFP32_18:
+            return launch_split_halo_typed<FieldF18>(stage, uin, uout, z, h, g, eps, lower_out, lower_v, lower_t,
+                                                     upper_out, upper_v, st);
+        case kFP32_12:
+            return launch_split_halo_typed<FieldF12>(stage, uin, uout, z, h, g, eps, lower_out, lower_v, lower_t,
+                                                     upper_out, upper_v, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -34,6 +34,18 @@ cudaError_t launch_rk_stage(int prec, int stage, const void* uin, void* uout, vo
 cudaError_t launch_plaq_field(int prec, const void* u, void* h, const Geo& g, cudaStream_t st);
 cudaError_t launch_rk_split_stage(int prec, int stage, const void* uin, void* uout, void* z, const void* h,
                                   const Geo& g, double eps, cudaStream_t st);
+// Its slab form with the halo stores of launch_rk_stage_halo (h must hold the
+// plane generators of local slices 0..nt, see plaq_range).
+cudaError_t launch_rk_split_stage_halo(int prec, int stage, const void* uin, void* uout, void* z, const void* h,
+                                       const Geo& g, double eps, void* lower_out, int lower_v, int lower_t,
+                                       void* upper_out, int upper_v, cudaStream_t st);
+// The sites whose plane generators a stage reads: a slab's links of slice 1
+// read those of halo slice 0, so its range starts there (g.site0 = one slice).
+inline Geo plaq_range(const Geo& g, bool slab) {
+    Geo p = g;
+    if (slab) p.site0 = 0;
+    return p;
+}
 
 // The same stage for a time slab (g.site0 = sites per slice, interior slices
 // [1, nt]): each new link of local slice 1 is also stored into the lower slab's

@@ -278,6 +278,7 @@ int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nstep
     for (int i = 0; i < n; i++) {
         const ymflow_ctx* c = ctxs[i];
         if (!c->slab || c->comm) return fail(c0, YMFLOW_ERR_ARG, "every context must be an unconnected slab");
+        if (c->stage_form != c0->stage_form) return fail(c0, YMFLOW_ERR_ARG, "slabs with different stage forms");
         if (c->prec != c0->prec || std::memcmp(c->gdims, c0->gdims, sizeof(c->gdims)) != 0)
             return fail(c0, YMFLOW_ERR_ARG, "slabs of different configurations or precisions");
         if (c->t0 != t) return fail(c0, YMFLOW_ERR_ARG, "slabs must tile the time extent in order");
@@ -341,10 +342,20 @@ int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nstep
                     ymflow_ctx* lo = ctxs[(i + n - 1) % n];
                     ymflow_ctx* hi = ctxs[(i + 1) % n];
                     DeviceGuard g(c->device);
-                    YM_CK(c, launch_rk_stage_halo(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z, c->geo, eps,
-                                                  lo->u[1 - lo->cur], lo->geo.V, lo->nt + 1, hi->u[1 - hi->cur],
-                                                  hi->geo.V, c->stream),
-                          "stage launch");
+                    if (c->stage_form == 1) {
+                        YM_CK(c, launch_plaq_field(c->prec, c->u[c->cur], c->hfield, plaq_range(c->geo, true),
+                                                   c->stream),
+                              "plaquette-field launch");
+                        YM_CK(c, launch_rk_split_stage_halo(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z,
+                                                            c->hfield, c->geo, eps, lo->u[1 - lo->cur], lo->geo.V,
+                                                            lo->nt + 1, hi->u[1 - hi->cur], hi->geo.V, c->stream),
+                              "stage launch");
+                    } else {
+                        YM_CK(c, launch_rk_stage_halo(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z, c->geo,
+                                                      eps, lo->u[1 - lo->cur], lo->geo.V, lo->nt + 1,
+                                                      hi->u[1 - hi->cur], hi->geo.V, c->stream),
+                              "stage launch");
+                    }
                 }
                 for (int i = 0; i < n; i++) ctxs[i]->cur = 1 - ctxs[i]->cur;
                 if ((r = group_order(ctxs, n, evs.ev)) != YMFLOW_OK) return r;
@@ -352,9 +363,18 @@ int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nstep
                 for (int i = 0; i < n; i++) {
                     ymflow_ctx* c = ctxs[i];
                     DeviceGuard g(c->device);
-                    YM_CK(c, launch_rk_stage(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z, c->geo, eps,
-                                             c->block, c->stream),
-                          "stage launch");
+                    if (c->stage_form == 1) {
+                        YM_CK(c, launch_plaq_field(c->prec, c->u[c->cur], c->hfield, plaq_range(c->geo, true),
+                                                   c->stream),
+                              "plaquette-field launch");
+                        YM_CK(c, launch_rk_split_stage(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z,
+                                                       c->hfield, c->geo, eps, c->stream),
+                              "stage launch");
+                    } else {
+                        YM_CK(c, launch_rk_stage(c->prec, stage, c->u[c->cur], c->u[1 - c->cur], c->z, c->geo, eps,
+                                                 c->block, c->stream),
+                              "stage launch");
+                    }
                     c->cur = 1 - c->cur;
                 }
                 if ((r = exchange_current()) != YMFLOW_OK) return r;

@@ -141,12 +141,20 @@ int run_step_slab(ymflow_ctx* c, double eps, cudaEvent_t* ev) {
     const int from = c->cur;
     const int in[3] = {from, 1 - from, from};
     for (int s = 0; s < 3; s++) {
-        if (ev) {
-            cudaEventRecord(ev[3 * s], c->stream);
-            cudaEventRecord(ev[3 * s + 1], c->stream);
+        if (ev) cudaEventRecord(ev[3 * s], c->stream);
+        if (c->stage_form == 1) {
+            YM_CK(c, launch_plaq_field(c->prec, c->u[in[s]], c->hfield, plaq_range(c->geo, true), c->stream),
+                  "plaquette-field launch");
+            if (ev) cudaEventRecord(ev[3 * s + 1], c->stream);
+            YM_CK(c, launch_rk_split_stage(c->prec, s, c->u[in[s]], c->u[1 - in[s]], c->z, c->hfield, c->geo, eps,
+                                           c->stream),
+                  "stage launch");
+        } else {
+            if (ev) cudaEventRecord(ev[3 * s + 1], c->stream);
+            YM_CK(c, launch_rk_stage(c->prec, s, c->u[in[s]], c->u[1 - in[s]], c->z, c->geo, eps, c->block,
+                                     c->stream),
+                  "stage launch");
         }
-        YM_CK(c, launch_rk_stage(c->prec, s, c->u[in[s]], c->u[1 - in[s]], c->z, c->geo, eps, c->block, c->stream),
-              "stage launch");
         if (ev) cudaEventRecord(ev[3 * s + 2], c->stream);
         const int r = slab_exchange(c, 1 - in[s]);
         if (r != YMFLOW_OK) return r;
@@ -353,13 +361,6 @@ ymflow_ctx* ymflow_create_slab(const int global_dims[4], int t0, int nt, int pre
     if (!c) return nullptr;
     c->slab = true;
     c->geo.tile_groups = 0;  // the interior range starts at a halo slice: plain order
-    if (c->hfield) {  // slabs flow with the fused stage kernels (the halo stores are fused there)
-        DeviceGuard guard(device);
-        cudaFree(c->hfield);
-        c->bytes -= int64_t(plane_field_bytes(c->prec, c->geo.V));
-        c->hfield = nullptr;
-    }
-    c->stage_form = 0;
     c->t0 = t0;
     c->nt = nt;
     for (int i = 0; i < 4; i++) c->gdims[i] = global_dims[i];
@@ -773,7 +774,6 @@ int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
             return YMFLOW_OK;
         case YMFLOW_OPT_STAGE_FORM: {
             if (value != 0 && value != 1) return fail(c, YMFLOW_ERR_ARG, "stage form is 0 (fused) or 1 (two kernels)");
-            if (value == 1 && c->slab) return fail(c, YMFLOW_ERR_STATE, "slabs flow with the fused stage kernel");
             DeviceGuard guard(c->device);
             if (value == 1 && !c->hfield) {
                 const int r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, c->geo.V), "plaquette field");

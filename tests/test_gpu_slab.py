@@ -11,10 +11,11 @@ N8 = (8, 4, 4, 10)  # spatial volume 128 (whole warp groups), 10 time slices
 
 
 def whole(precision, n=N8, seed=11, steps=6, every=2):
-    from latticeyangmills_b200 import GluonField, _native as N
+    # slabs and the whole lattice run the same stage form (fused in FP64, the
+    # two-kernel stage in FP32)
+    from latticeyangmills_b200 import GluonField
 
     with GluonField(n, precision) as f:
-        f.set_option(N.OPT_STAGE_FORM, 0)  # slabs run the fused stage kernel: compare like with like
         f.init_links("expiah", 0.4, seed)
         U0 = f.download()
         rows = f.flow(0.02, steps, every, reunit_every=3 if precision != "fp64" else 0)

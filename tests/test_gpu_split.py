@@ -73,9 +73,56 @@ def test_stage_form_defaults_and_refusals():
             with pytest.raises(YmflowError):
                 f.set_option(N.OPT_STAGE_FORM, 2)
     with GluonField.slab((8, 4, 4, 10), 0, 5, "fp32_18") as s:
-        assert s.get_option(N.OPT_STAGE_FORM) == 0  # slabs store their halos from the fused kernel
+        assert s.get_option(N.OPT_STAGE_FORM) == 1
+        s.set_option(N.OPT_STAGE_FORM, 0)
+        assert s.get_option(N.OPT_STAGE_FORM) == 0
+
+
+def test_slab_group_needs_one_stage_form():
+    from latticeyangmills_b200 import GluonField, YmflowError, _native as N, slab_group_flow
+
+    a = GluonField.slab((8, 4, 4, 10), 0, 5, "fp32_12")
+    b = GluonField.slab((8, 4, 4, 10), 5, 5, "fp32_12")
+    try:
+        for sl in (a, b):
+            sl.init_links("expiah", 0.4, 3)
+        b.set_option(N.OPT_STAGE_FORM, 0)
         with pytest.raises(YmflowError):
-            s.set_option(N.OPT_STAGE_FORM, 1)
+            slab_group_flow([a, b], 0.02, 2, 1)
+        b.set_option(N.OPT_STAGE_FORM, 1)
+        rows = slab_group_flow([a, b], 0.02, 2, 1)
+        assert rows.shape[0] == 3
+    finally:
+        a.close()
+        b.close()
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_fp32_slabs_in_both_forms_match_the_whole_lattice(form):
+    """Three FP32 slabs flowing together (the two-kernel stage stores its
+    boundary links into the neighbours' halos as the fused one does) against
+    the whole lattice in the same form: equal to FP32 rounding."""
+    from latticeyangmills_b200 import GluonField, _native as N, slab_group_flow
+
+    n = (8, 4, 4, 10)
+    with GluonField(n, "fp32_12") as f:
+        f.set_option(N.OPT_STAGE_FORM, form)
+        f.init_links("expiah", 0.4, 5)
+        want = f.flow(0.02, 6, 3, reunit_every=3)
+        want_links = f.download()
+    slabs = [GluonField.slab(n, t0, nt, "fp32_12") for t0, nt in ((0, 4), (4, 3), (7, 3))]
+    try:
+        for sl in slabs:
+            sl.set_option(N.OPT_STAGE_FORM, form)
+            sl.init_links("expiah", 0.4, 5)
+        got = slab_group_flow(slabs, 0.02, 6, 3, reunit_every=3)
+        links = np.concatenate([sl.download() for sl in slabs])
+    finally:
+        for sl in slabs:
+            sl.close()
+    assert np.abs(links - want_links).max() < 1e-5
+    np.testing.assert_array_equal(got[:, :2], want[:, :2])
+    np.testing.assert_allclose(got[:, [2, 4, 5]], want[:, [2, 4, 5]], rtol=1e-6)
 
 
 def test_switching_forms_mid_flow_continues_the_flow():
