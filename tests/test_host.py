@@ -136,3 +136,23 @@ def test_reference_registry_reaches_the_gpu_wilsonflow(tmp_path):
     res = subprocess.run([str(REF_GPU_APP), str(run)], capture_output=True, text=True)
     assert res.returncode == 1
     assert "ymflow create" in res.stderr
+
+
+def test_bench_byte_accounting_and_profiled_traffic():
+    """The roofline numerators of bench.py: the fused stage's compulsory bytes
+    per link-update, the two-kernel stage's per kernel, and the DRAM traffic
+    scaled from the committed ncu summaries."""
+    import bench
+
+    assert [bench.bytes_per_link_update(p) for p in ("fp64", "fp32_18", "fp32_12")] == [1120, 560, 416]
+    field, stage = bench.split_bytes_per_link("fp32_12")
+    assert field == 96 and stage == pytest.approx(186.6667, rel=1e-5)
+    assert 3 * (field + stage) == pytest.approx(848)
+    field, stage = bench.split_bytes_per_link("fp32_18")
+    assert field == 120 and 3 * (field + stage) == pytest.approx(1064)
+    alg = 1e9
+    got = bench.profiled_traffic("fp32_12", (32, 32, 32, 32), alg, "rk_split_stage")
+    assert got == pytest.approx(843941120 / 872415232 * alg)
+    got = bench.profiled_traffic("fp32_12", (32, 32, 32, 32), alg, "plaq_field")
+    assert got == pytest.approx(372003840 / 402653184 * alg)
+    assert bench.profiled_traffic("fp32_12", (16, 16, 16, 16), alg, "rk_split_stage") is None
