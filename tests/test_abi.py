@@ -44,8 +44,8 @@ def test_status_and_enum_values_match_header():
     assert (d["YMFLOW_FP64"], d["YMFLOW_FP32_18"], d["YMFLOW_FP32_12"]) == (N.FP64, N.FP32_18, N.FP32_12)
     assert (d["YMFLOW_FIELD_COLD"], d["YMFLOW_FIELD_EXPIAH"], d["YMFLOW_FIELD_HOT"], d["YMFLOW_FIELD_CURRENT"]) == (
         N.FIELD_COLD, N.FIELD_EXPIAH, N.FIELD_HOT, N.FIELD_CURRENT)
-    assert (d["YMFLOW_OPT_BLOCK"], d["YMFLOW_OPT_GRAPH"], d["YMFLOW_OPT_OBS_BLOCK"]) == (
-        N.OPT_BLOCK, N.OPT_GRAPH, N.OPT_OBS_BLOCK)
+    assert (d["YMFLOW_OPT_BLOCK"], d["YMFLOW_OPT_GRAPH"], d["YMFLOW_OPT_OBS_BLOCK"], d["YMFLOW_OPT_STAGE_FORM"]) == (
+        N.OPT_BLOCK, N.OPT_GRAPH, N.OPT_OBS_BLOCK, N.OPT_STAGE_FORM)
 
 
 def test_obs_struct_layout():

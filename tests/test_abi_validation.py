@@ -58,6 +58,10 @@ def test_calls_without_a_context_or_buffer():
         args = [None] * len(getattr(lib, fn).argtypes)
         assert getattr(lib, fn)(*args) == N.ERR_ARG, fn
     assert lib.ymflow_set_time(None, 0, 0.0) == N.ERR_ARG
+    assert lib.ymflow_set_option(None, N.OPT_STAGE_FORM, 1) == N.ERR_ARG
+    ms = ctypes.c_float()
+    assert lib.ymflow_time_steps(None, 0.01, 1, ctypes.byref(ms), None) == N.ERR_ARG
+    assert lib.ymflow_time_kernels(None, 0.01, 1, ctypes.byref(ms), None, None) == N.ERR_ARG
     assert lib.ymflow_load_file(None, b"x", 0, 0) == N.ERR_ARG
     assert lib.ymflow_slab_group_flow(None, 0, 0.01, 1, 0, 0, None, 0, None) == N.ERR_ARG
 
