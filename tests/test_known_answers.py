@@ -58,3 +58,56 @@ def test_flow_raises_the_plaquette(oracle):
     U = oracle.gen_expiah(n, 0.35, 3, 0)
     rows = oracle.flow(U, n, 0.02, 40, 1)
     assert np.all(np.diff(rows[:, 2]) > 0)
+
+
+def _cplx(a):
+    """(..., 18) doubles, row-major (re, im) -> (..., 3, 3) complex."""
+    return (a[..., 0::2] + 1j * a[..., 1::2]).reshape(a.shape[:-1] + (3, 3))
+
+
+@pytest.mark.parametrize("n", [(4, 4, 4, 4), (3, 4, 5, 6)])
+def test_plaquette_field_form_of_the_force(oracle, n):
+    """The identity the two-kernel stage computes:
+    D_mu(x) = sum_{nu != mu} s_{mu nu} [H_p(x) - U_nu(x-nu)^+ H_p(x-nu) U_nu(x-nu)],
+    with H_p = (i/2)[P_p - P_p^+]_TL of the plaquette P_ab(x) = U_a(x) U_b(x+a)
+    U_a(x+b)^+ U_b(x)^+ (a < b) and s = +1 for mu < nu, -1 otherwise, against the
+    oracle's staple form of the reference's computeDerivative, in FP64."""
+    U = _cplx(oracle.gen_expiah(n, 0.4, 3))  # (t, z, y, x, mu, 3, 3)
+    axis = {0: 3, 1: 2, 2: 1, 3: 0}  # direction -> array axis (x fastest)
+
+    def up(a, d):  # a(x + d)
+        return np.roll(a, -1, axis=axis[d])
+
+    def down(a, d):  # a(x - d)
+        return np.roll(a, 1, axis=axis[d])
+
+    dag = lambda m: np.conj(np.swapaxes(m, -1, -2))
+
+    def herm(x):  # (i/2)[X - X^+]_TL
+        a = x - dag(x)
+        a = a - np.trace(a, axis1=-2, axis2=-1)[..., None, None] / 3 * np.eye(3)
+        return 0.5j * a
+
+    planes = [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
+    H = {}
+    for a, b in planes:
+        ua, ub = U[..., a, :, :], U[..., b, :, :]
+        H[a, b] = herm(ua @ up(ub, a) @ dag(up(ua, b)) @ dag(ub))
+    for mu in range(4):
+        d = 0
+        for nu in range(4):
+            if nu == mu:
+                continue
+            h = H[min(mu, nu), max(mu, nu)]
+            v = down(U[..., nu, :, :], nu)
+            d = d + (1 if mu < nu else -1) * (h - dag(v) @ down(h, nu) @ v)
+        want = _cplx(oracle.derivative(oracle_field(U, n), n, mu)).reshape(d.shape)
+        assert np.abs(d - want).max() < 1e-13, mu
+
+
+def oracle_field(Uc, n):
+    """(t, z, y, x, mu, 3, 3) complex -> the oracle's (t, z, y, x, mu, 18) doubles."""
+    out = np.empty(Uc.shape[:-2] + (18,))
+    out[..., 0::2] = Uc.real.reshape(Uc.shape[:-2] + (9,))
+    out[..., 1::2] = Uc.imag.reshape(Uc.shape[:-2] + (9,))
+    return np.ascontiguousarray(out)
