@@ -204,17 +204,44 @@ YMFLOW_API int ymflow_time_kernels(ymflow_ctx* ctx, double eps, int nsteps, floa
  * threads per block of the observables kernel (192: six warps, one per
  * plane, per 32 sites; read-only in effect, other values are rejected);
  * YMFLOW_OPT_GRAPH: 1 = replay each RK3 step as a captured CUDA graph
- * (default), 0 = plain launches; YMFLOW_OPT_STAGE_FORM: 0 = one fused kernel
- * per RK3 stage (the FP64 default), 1 = two kernels per stage, the six
- * plaquettes' generators of every site into a stored field (6 x 8 reals per
- * site of device memory) and each link's force from them (the FP32 default).
+ * (default), 0 = plain launches; YMFLOW_OPT_STAGE_FORM: the kernels of one RK3
+ * stage (the reference's computeDerivative + exp + link update for all mu,
+ * src/Apps/wilsonflow.cpp:143-171):
+ *   0 = one fused kernel, staples summed per link (the FP64 default);
+ *   1 = two kernels, the six plaquettes' generators of every site into a
+ *       stored field (6 x 8 reals per site of device memory), then each link's
+ *       force from them (FP32 default where form 2 has no tiling, and slabs);
+ *   2 = one kernel: blocks of Lx x ty x tz sites of a time slice compute their
+ *       plaquette generators into shared memory, recompute the lower (y, z)
+ *       faces, stream along t and finish the links from there (the FP32
+ *       default where the lattice tiles into at least one block per SM;
+ *       whole-lattice contexts only).
+ * YMFLOW_OPT_TILE: form 2's tile, value = (ty << 16) | tz; ty must divide the
+ * y extent, tz the z extent, Lx ty must be a multiple of 32 and Lx ty tz within
+ * 64..512 (YMFLOW_ERR_ARG otherwise).  YMFLOW_OPT_TIMED_REUNIT: the FP64
+ * reunitarisation of the mixed forms after every n-th step of
+ * ymflow_time_steps / ymflow_time_kernels (0 = none, the default), so timed
+ * steps can carry it as ymflow_flow's reunit_every does.
  * Slabs flowing together (ymflow_slab_group_flow) must share one form. */
 #define YMFLOW_OPT_BLOCK 1
 #define YMFLOW_OPT_GRAPH 2
 #define YMFLOW_OPT_OBS_BLOCK 3
 #define YMFLOW_OPT_STAGE_FORM 4
+#define YMFLOW_OPT_TILE 5
+#define YMFLOW_OPT_TIMED_REUNIT 6
 YMFLOW_API int ymflow_set_option(ymflow_ctx* ctx, int key, int64_t value);
 YMFLOW_API int ymflow_get_option(const ymflow_ctx* ctx, int key, int64_t* value);
+
+/* The project's autotuner for one context (no counterpart in the reference,
+ * whose stage is a fixed sequence of whole-lattice passes,
+ * src/Apps/wilsonflow.cpp:141-172): times one RK3 stage in every form and
+ * tiling the lattice allows (form 0, form 1, form 2 at every valid (ty, tz)),
+ * keeps the fastest, and caches the choice for every context of the same
+ * extents, precision and device in the process.  The current links are not
+ * changed (stage 0 runs into the other buffer).  Forms agree to rounding, so
+ * a tuned flow can differ from the default one in the last bits.  Writes the
+ * chosen form and tile (0, 0 unless form 2).  Not for slab contexts. */
+YMFLOW_API int ymflow_autotune(ymflow_ctx* ctx, double eps, int* stage_form, int* tile_y, int* tile_z);
 
 /* --- One configuration split along t over several GPUs -------------------- */
 /* A slab context holds the time slices [t0, t0 + nt) of a configuration of
@@ -291,11 +318,14 @@ YMFLOW_API int ymflow_device_bytes(const ymflow_ctx* ctx, int64_t* bytes);
  * stream) of the current device.  Allocates nothing: its scratch is a fixed
  * 1.5 MB device array inside the library (held by every GPU that loads it),
  * which limits the lattice to YMFLOW_NOALLOC_MAX_SITES sites; larger lattices
- * return YMFLOW_ERR_CAPACITY.  The first call on a device looks the array's
- * device address up once and should come before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race and must be ordered by
- * the caller.  Returns YMFLOW_ERR_ARG, YMFLOW_ERR_CAPACITY, YMFLOW_ERR_NODEVICE
- * or YMFLOW_ERR_CUDA (launch failure) on error. */
+ * return YMFLOW_ERR_CAPACITY.  links_aos_device must be 16-byte aligned and
+ * out_device 8-byte aligned (YMFLOW_ERR_ARG otherwise, before any launch).
+ * The first call on a device looks the array's device address up once and
+ * should come before any stream capture; the cached address does not survive
+ * a cudaDeviceReset.  All calls share the array: calls that overlap on the GPU
+ * race and must be ordered by the caller.  Returns YMFLOW_ERR_ARG,
+ * YMFLOW_ERR_CAPACITY, YMFLOW_ERR_NODEVICE or YMFLOW_ERR_CUDA (launch failure)
+ * on error. */
 #define YMFLOW_NOALLOC_MAX_SITES 8388608
 YMFLOW_API int ymflow_observables_noalloc(const double* links_aos_device, const int dims[4], double* out_device,
                                           void* stream);

@@ -29,7 +29,8 @@ PRECISIONS = {"fp64": FP64, "fp32_18": FP32_18, "fp32_12": FP32_12}
 FIELD_COLD, FIELD_EXPIAH, FIELD_HOT, FIELD_CURRENT = 0, 1, 2, 3
 IO_BIG_ENDIAN = 1
 NCCL_ID_BYTES = 128
-OPT_BLOCK, OPT_GRAPH, OPT_OBS_BLOCK, OPT_STAGE_FORM = 1, 2, 3, 4
+OPT_BLOCK, OPT_GRAPH, OPT_OBS_BLOCK, OPT_STAGE_FORM, OPT_TILE, OPT_TIMED_REUNIT = 1, 2, 3, 4, 5, 6
+STAGE_FUSED, STAGE_SPLIT, STAGE_TILE = 0, 1, 2
 
 # every symbol include/ymflow.h declares
 EXPORTS = (
@@ -38,6 +39,7 @@ EXPORTS = (
     "ymflow_init_links",
     "ymflow_generate_metropolis", "ymflow_observables", "ymflow_flow", "ymflow_derivative", "ymflow_su3_exp",
     "ymflow_reset_time", "ymflow_set_time", "ymflow_time_steps", "ymflow_time_kernels", "ymflow_set_option", "ymflow_get_option",
+    "ymflow_autotune",
     "ymflow_host_alloc", "ymflow_host_free", "ymflow_device_bytes", "ymflow_fma_peak",
     "ymflow_ensemble_create", "ymflow_ensemble_destroy", "ymflow_ensemble_last_error",
     "ymflow_ensemble_upload", "ymflow_ensemble_download", "ymflow_ensemble_init_links",
@@ -114,6 +116,8 @@ def load():
                                       ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
     l.ymflow_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_int64]
     l.ymflow_get_option.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    l.ymflow_autotune.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int)]
     l.ymflow_host_alloc.argtypes = [ctypes.c_int64, ctypes.POINTER(vp)]
     l.ymflow_host_free.argtypes = [vp]
     l.ymflow_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]

@@ -22,7 +22,11 @@ struct ymflow_ctx {
     int cur = 0;                      // which of u[] holds the current field
     void* z = nullptr;                // RK generator, 8 reals per link
     void* hfield = nullptr;           // plaquette field of the two-kernel stage (stage_form 1)
-    int stage_form = 0;               // 0: fused stage kernel, 1: plaquette field + stage kernel
+    int stage_form = 0;               // 0: fused stage kernel, 1: plaquette field + stage kernel,
+                                      // 2: one kernel with the tile's plaquette field in shared memory
+    ym::TileShape tile{};             // stage form 2's tiling (valid when tile_ok)
+    bool tile_ok = false;
+    int timed_reunit = 0;             // time_steps / time_kernels: reunitarise every n-th step (0: never)
     double* staging = nullptr;        // .bin-layout device buffer for upload/download
     size_t staging_bytes = 0;
     double* partials = nullptr;       // observables: 3 doubles per block

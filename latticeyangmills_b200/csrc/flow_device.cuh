@@ -174,15 +174,15 @@ __device__ __forceinline__ void rk_link_update(const F& in, const F& out, const 
 // plane index of directions a < b: (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) -> 0..5
 __device__ __forceinline__ int plane_index(int a, int b) { return a * (5 - a) / 2 + b - 1; }
 
-// H_p(x) of plane p at site s into hf.
+// directions a < b of plane p
+__device__ __forceinline__ int plane_a(int p) { return p < 3 ? 0 : (p < 5 ? 1 : 2); }
+__device__ __forceinline__ int plane_b(int p) { return p < 3 ? p + 1 : (p < 5 ? p - 1 : 3); }
+
+// H_ab(x) = (i/2)[P_ab(x) - P_ab(x)^+]_TL at site s with coordinates c.
 template <class F>
-__device__ __forceinline__ void plaq_plane(const F& u, const ForceField<typename F::Real>& hf, const Geo& g, int s,
-                                           int p) {
+__device__ __forceinline__ Herm8<typename F::Real> plane_generator(const F& u, const Geo& g, int s, const int c[4],
+                                                                   int a, int b) {
     using R = typename F::Real;
-    const int a = p < 3 ? 0 : (p < 5 ? 1 : 2);
-    const int b = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
-    int c[4];
-    g.coords(s, c);
     const int s_pa = g.hop_rt(s, g.coord(c, a), a, +1);
     const int s_pb = g.hop_rt(s, g.coord(c, b), b, +1);
     M3<R> lo, up;  // U_a(x) U_b(x+a) and U_b(x) U_a(x+b): P = lo up^+
@@ -196,7 +196,16 @@ __device__ __forceinline__ void plaq_plane(const F& u, const ForceField<typename
         const M3<R> y = u.load(a, s_pb);
         mmul<false, false>(x, y, up);
     }
-    hf.store(p, s, force_from_b_cdag(lo, up));
+    return force_from_b_cdag(lo, up);
+}
+
+// H_p(x) of plane p at site s into hf.
+template <class F>
+__device__ __forceinline__ void plaq_plane(const F& u, const ForceField<typename F::Real>& hf, const Geo& g, int s,
+                                           int p) {
+    int c[4];
+    g.coords(s, c);
+    hf.store(p, s, plane_generator(u, g, s, c, plane_a(p), plane_b(p)));
 }
 
 // One link through one stage with its generator built from the plane field hf

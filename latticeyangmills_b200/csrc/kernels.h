@@ -39,6 +39,29 @@ cudaError_t launch_rk_split_stage(int prec, int stage, const void* uin, void* uo
 cudaError_t launch_rk_split_stage_halo(int prec, int stage, const void* uin, void* uout, void* z, const void* h,
                                        const Geo& g, double eps, void* lower_out, int lower_v, int lower_t,
                                        void* upper_out, int upper_v, cudaStream_t st);
+// The same stage in one kernel with the plane generators of a tile of sites in
+// shared memory (flow_tile.cu): tiles of whole x lines x ty x tz (y, z) of one
+// time slice, one thread per site, each block streaming along t through a run
+// of (tile column, t) units.
+struct TileShape {
+    int ty, tz;      // tile extent in y and z
+    int ns;          // sites per tile = threads per block (Lx ty tz)
+    int nyt, nzt;    // tiles along y and z
+    int nfy, nfz;    // sites of the recomputed lower y / z faces (0: the tile spans the extent)
+    int units;       // tile columns x time slices
+    int grid;        // blocks (persistent: min(units, SMs x resident blocks))
+};
+// Whether (ty, tz) tiles the whole-lattice geometry g (whole warps per x-y run,
+// 64..512 threads, shared memory within 227 KB); fills *out (grid left 0).
+bool make_tile_shape(int prec, const Geo& g, int ty, int tz, TileShape* out);
+size_t tile_smem_bytes(int prec, const TileShape& tp);
+// Opt the tile kernels of a precision into their shared memory (per device).
+cudaError_t prepare_tile_kernels(int prec);
+// tp->grid for `device` from the kernel's occupancy.
+cudaError_t tile_grid(int prec, int device, TileShape* tp);
+cudaError_t launch_rk_tile_stage(int prec, int stage, const void* uin, void* uout, void* z, const Geo& g,
+                                 const TileShape& tp, double eps, cudaStream_t st);
+
 // The sites whose plane generators a stage reads: a slab's links of slice 1
 // read those of halo slice 0, so its range starts there (g.site0 = one slice).
 inline Geo plaq_range(const Geo& g, bool slab) {

@@ -17,7 +17,15 @@
 // array's name to a kernel (in host code it names a host-side stand-in), so
 // on the first call on each device, with that device current, the device
 // address is fetched once with cudaGetSymbolAddress and cached.  Make that
-// first call before any stream capture.
+// first call before any stream capture.  The cache lives as long as the
+// process's CUDA context: after a cudaDeviceReset the library must be
+// reloaded before this entry point is used again.
+//
+// The links are read as 16-byte vectors and the results written as doubles,
+// so the links must start on a 16-byte boundary and the output on an 8-byte
+// one; a caller passing an offset into its own pool (one link is 144 bytes,
+// a site 576) gets YMFLOW_ERR_ARG for an unaligned pointer before anything is
+// launched, instead of a misaligned-address fault that would end its context.
 //
 // Every call shares the array.  Each block writes (never accumulates) its own
 // partial and the fold reads only the partials written by the same call, so
@@ -27,6 +35,7 @@
 // must be ordered by the caller.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "kernels.h"
@@ -101,6 +110,8 @@ extern "C" int ymflow_observables_noalloc(const double* links_aos_device, const 
         v *= dims[i];
         if (v > YMFLOW_NOALLOC_MAX_SITES) return YMFLOW_ERR_CAPACITY;
     }
+    if (reinterpret_cast<uintptr_t>(links_aos_device) % 16 != 0 || reinterpret_cast<uintptr_t>(out_device) % 8 != 0)
+        return YMFLOW_ERR_ARG;
     int device = -1;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kNoAllocMaxDevices) {
         cudaGetLastError();

@@ -5,7 +5,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -101,6 +104,38 @@ int ensure_meas(ymflow_ctx* c, int rows) {
 
 namespace {
 
+// The tiling of the shared-memory stage kernel used by default: among the
+// (ty, tz) that tile the lattice into at least one unit per SM, the one with
+// the least recomputed face work per site (ties: the smaller tile).  false if
+// none qualifies (small lattices, x extents whose lines do not fill whole
+// warps, slabs).
+bool default_tile(const ymflow_ctx* c, TileShape* out) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    bool found = false;
+    double best = 0.0;
+    for (int ty = 1; ty <= c->geo.n[1]; ty++) {
+        for (int tz = 1; tz <= c->geo.n[2]; tz++) {
+            TileShape tp;
+            if (!make_tile_shape(c->prec, c->geo, ty, tz, &tp) || tp.units < sms) continue;
+            const double cost = double(tp.nfy + tp.nfz) / tp.ns + 1e-6 * tp.ns;
+            if (!found || cost < best) {
+                if (tile_grid(c->prec, c->device, &tp) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                *out = tp;
+                best = cost;
+                found = true;
+            }
+        }
+    }
+    return found;
+}
+
 void drop_graphs(ymflow_ctx* c) {
     for (int i = 0; i < 2; i++) {
         if (c->graph[i]) cudaGraphExecDestroy(c->graph[i]);
@@ -125,6 +160,9 @@ cudaError_t enqueue_step(ymflow_ctx* c, int from, double eps, cudaEvent_t* ev) {
             if (e != cudaSuccess) return e;
             if (ev) cudaEventRecord(ev[3 * s + 1], c->stream);
             e = launch_rk_split_stage(c->prec, s, in[s], out[s], c->z, c->hfield, c->geo, eps, c->stream);
+        } else if (c->stage_form == 2) {
+            if (ev) cudaEventRecord(ev[3 * s + 1], c->stream);
+            e = launch_rk_tile_stage(c->prec, s, in[s], out[s], c->z, c->geo, c->tile, eps, c->stream);
         } else {
             if (ev) cudaEventRecord(ev[3 * s + 1], c->stream);
             e = launch_rk_stage(c->prec, s, in[s], out[s], c->z, c->geo, eps, c->block, c->stream);
@@ -307,14 +345,24 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->u[1], ub, "link buffer 1");
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->z, zb, "force buffer");
     if (r == YMFLOW_OK) r = dev_alloc(c, (void**)&c->deviation, sizeof(unsigned long long), "drift flag");
-    // FP32 forms flow with the two-kernel stage (plaquette field, then the
-    // stage): fewer multiply-adds per link for twice the stage's bytes, which
-    // the FP32 kernels have room for (0.98 against 1.17 ms per step at 32^4 for
-    // the 12-real form against the fused 18-real one).  FP64 keeps the fused
-    // kernel, the faster form at its two-row staple products.
+    // FP32 forms flow with the plaquette-field form of the force (fewer
+    // multiply-adds per link than the staple form): in one kernel with a
+    // tile's plane generators in shared memory where the lattice tiles into
+    // enough blocks to fill the GPU, else as two kernels through a stored
+    // plaquette field.  FP64 keeps the fused staple kernel, the faster form at
+    // its two-row staple products.  ymflow_autotune times every form.
+    if (r == YMFLOW_OK && prepare_tile_kernels(c->prec) != cudaSuccess) {
+        const cudaError_t e = cudaGetLastError();
+        r = cuda_fail(c, e == cudaSuccess ? cudaErrorInvalidValue : e, "tile kernel set-up");
+    }
+    if (r == YMFLOW_OK) c->tile_ok = default_tile(c, &c->tile);
     if (r == YMFLOW_OK && c->prec != YMFLOW_FP64) {
-        r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, V), "plaquette field");
-        c->stage_form = 1;
+        if (c->tile_ok) {
+            c->stage_form = 2;
+        } else {
+            r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, V), "plaquette field");
+            c->stage_form = 1;
+        }
     }
     if (r == YMFLOW_OK) r = ensure_partials(c);
     if (r == YMFLOW_OK) r = ensure_meas(c, 16);
@@ -369,6 +417,20 @@ ymflow_ctx* ymflow_create_slab(const int global_dims[4], int t0, int nt, int pre
     c->geo.global0 = int64_t(t0) * vs;
     c->geo.vglobal = vs * global_dims[3];
     c->use_graph = false;
+    // slabs flow with the two-kernel stage (FP32) or the fused kernel (FP64):
+    // the tile kernel covers whole-lattice contexts only
+    c->tile_ok = false;
+    if (c->stage_form == 2) {
+        DeviceGuard guard(device);
+        const int r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, c->geo.V), "plaquette field");
+        if (r != YMFLOW_OK) {
+            if (status) *status = r;
+            g_create_error = c->err;
+            ymflow_destroy(c);
+            return nullptr;
+        }
+        c->stage_form = 1;
+    }
     return c;
 }
 
@@ -726,12 +788,15 @@ int ymflow_time_kernels(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms
         YM_CK(c, cudaEventCreate(&e), "event create");
         c->events.push_back(e);
     }
+    const bool reunit = c->prec != YMFLOW_FP64 && c->timed_reunit > 0;
     YM_CK(c, cudaEventRecord(c->ev0, c->stream), "event record");
     for (int s = 0; s < nsteps; s++) {
         int r = run_step(c, eps, per_kernel ? c->events.data() + 9 * s : nullptr);
         if (r != YMFLOW_OK) return r;
         c->step++;
         c->t += eps;
+        if (reunit && (s + 1) % c->timed_reunit == 0)
+            YM_CK(c, launch_reunitarize(c->prec, c->u[c->cur], c->geo, c->deviation, c->stream), "reunitarise");
     }
     YM_CK(c, cudaEventRecord(c->ev1, c->stream), "event record");
     YM_CK(c, cudaEventSynchronize(c->ev1), "timed steps");
@@ -759,6 +824,113 @@ int ymflow_time_steps(ymflow_ctx* c, double eps, int nsteps, float* elapsed_ms, 
     return r;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Milliseconds per stage-0 launch in the context's current form, stage 0
+// running from the current links into the other buffer: the current field
+// is untouched and the generator buffer only written (every step's stage 0
+// writes it before stages 1 and 2 read it).
+int time_stage0(ymflow_ctx* c, double eps, int reps, float* ms) {
+    const void* a = c->u[c->cur];
+    void* b = c->u[1 - c->cur];
+    auto launch = [&]() -> cudaError_t {
+        if (c->stage_form == 1) {
+            cudaError_t e = launch_plaq_field(c->prec, a, c->hfield, c->geo, c->stream);
+            if (e != cudaSuccess) return e;
+            return launch_rk_split_stage(c->prec, 0, a, b, c->z, c->hfield, c->geo, eps, c->stream);
+        }
+        if (c->stage_form == 2) return launch_rk_tile_stage(c->prec, 0, a, b, c->z, c->geo, c->tile, eps, c->stream);
+        return launch_rk_stage(c->prec, 0, a, b, c->z, c->geo, eps, c->block, c->stream);
+    };
+    for (int i = 0; i < 2; i++) YM_CK(c, launch(), "autotune warm-up");
+    YM_CK(c, cudaEventRecord(c->ev0, c->stream), "event record");
+    for (int i = 0; i < reps; i++) YM_CK(c, launch(), "autotune launch");
+    YM_CK(c, cudaEventRecord(c->ev1, c->stream), "event record");
+    YM_CK(c, cudaEventSynchronize(c->ev1), "autotune timing");
+    YM_CK(c, cudaEventElapsedTime(ms, c->ev0, c->ev1), "elapsed time");
+    *ms /= float(reps);
+    return YMFLOW_OK;
+}
+
+struct TuneChoice {
+    int form, ty, tz;
+};
+std::mutex g_tune_mu;
+std::map<std::array<int, 6>, TuneChoice> g_tune_cache;  // (dims, precision, device) -> choice
+
+}  // namespace
+
+extern "C" {
+
+int ymflow_autotune(ymflow_ctx* c, double eps, int* stage_form, int* tile_y, int* tile_z) {
+    NvtxRange range("ymflow_autotune");
+    if (!c || !std::isfinite(eps)) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_autotune");
+    if (c->slab) return fail(c, YMFLOW_ERR_ARG, "slab contexts keep the stage form of their group");
+    if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
+    DeviceGuard guard(c->device);
+    YM_CK(c, cudaStreamSynchronize(c->stream), "autotune");
+    const std::array<int, 6> key = {c->dims[0], c->dims[1], c->dims[2], c->dims[3], c->prec, c->device};
+    auto apply = [&](const TuneChoice& ch) -> int {
+        if (ch.form == 2) {
+            const int r = ymflow_set_option(c, YMFLOW_OPT_TILE, (int64_t(ch.ty) << 16) | ch.tz);
+            if (r != YMFLOW_OK) return r;
+        }
+        return ymflow_set_option(c, YMFLOW_OPT_STAGE_FORM, ch.form);
+    };
+    auto report = [&]() {
+        if (stage_form) *stage_form = c->stage_form;
+        if (tile_y) *tile_y = c->stage_form == 2 ? c->tile.ty : 0;
+        if (tile_z) *tile_z = c->stage_form == 2 ? c->tile.tz : 0;
+    };
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            const int r = apply(it->second);
+            if (r == YMFLOW_OK) report();
+            return r;
+        }
+    }
+    const bool had_hfield = c->hfield != nullptr;
+    std::vector<TuneChoice> cands = {{0, 0, 0}, {1, 0, 0}};
+    for (int ty = 1; ty <= c->geo.n[1]; ty++)
+        for (int tz = 1; tz <= c->geo.n[2]; tz++) {
+            TileShape tp;
+            if (make_tile_shape(c->prec, c->geo, ty, tz, &tp)) cands.push_back({2, ty, tz});
+        }
+    TuneChoice best = {c->stage_form, c->tile.ty, c->tile.tz};
+    float best_ms = 0.f;
+    bool any = false;
+    for (const TuneChoice& ch : cands) {
+        int r = apply(ch);
+        if (r != YMFLOW_OK) continue;  // e.g. no device memory for the plaquette field
+        float ms = 0.f;
+        r = time_stage0(c, eps, 5, &ms);
+        if (r != YMFLOW_OK) return r;
+        if (!any || ms < best_ms) {
+            best = ch;
+            best_ms = ms;
+            any = true;
+        }
+    }
+    if (!any) return fail(c, YMFLOW_ERR_STATE, "autotune: no stage form could run");
+    int r = apply(best);
+    if (r != YMFLOW_OK) return r;
+    if (c->stage_form != 1 && !had_hfield && c->hfield) {  // drop the plaquette field tuning allocated
+        cudaFree(c->hfield);
+        c->bytes -= int64_t(plane_field_bytes(c->prec, c->geo.V));
+        c->hfield = nullptr;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    report();
+    return YMFLOW_OK;
+}
+
 int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
     if (!c) return YMFLOW_ERR_ARG;
     switch (key) {
@@ -773,7 +945,11 @@ int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
             c->use_graph = value != 0;
             return YMFLOW_OK;
         case YMFLOW_OPT_STAGE_FORM: {
-            if (value != 0 && value != 1) return fail(c, YMFLOW_ERR_ARG, "stage form is 0 (fused) or 1 (two kernels)");
+            if (value < 0 || value > 2)
+                return fail(c, YMFLOW_ERR_ARG, "stage form is 0 (fused), 1 (two kernels) or 2 (shared-memory tile)");
+            if (value == 2 && !c->tile_ok)
+                return fail(c, YMFLOW_ERR_ARG, "no tiling of this lattice for the shared-memory stage kernel "
+                                               "(set one with YMFLOW_OPT_TILE)");
             DeviceGuard guard(c->device);
             if (value == 1 && !c->hfield) {
                 const int r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, c->geo.V), "plaquette field");
@@ -786,6 +962,25 @@ int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
             c->stage_form = int(value);
             return YMFLOW_OK;
         }
+        case YMFLOW_OPT_TILE: {
+            const int ty = int(value >> 16), tz = int(value & 0xffff);
+            TileShape tp;
+            if (value < 0 || value > 0x7fffffff || !make_tile_shape(c->prec, c->geo, ty, tz, &tp))
+                return fail(c, YMFLOW_ERR_ARG, "tile (" + std::to_string(ty) + ", " + std::to_string(tz) +
+                                                   ") does not tile this lattice's (y, z) in whole warps of x lines "
+                                                   "within 64..512 threads and 227 KB of shared memory");
+            DeviceGuard guard(c->device);
+            YM_CK(c, tile_grid(c->prec, c->device, &tp), "tile occupancy");
+            YM_CK(c, cudaStreamSynchronize(c->stream), "tile switch");
+            drop_graphs(c);
+            c->tile = tp;
+            c->tile_ok = true;
+            return YMFLOW_OK;
+        }
+        case YMFLOW_OPT_TIMED_REUNIT:
+            if (value < 0 || value > (1 << 30)) return fail(c, YMFLOW_ERR_ARG, "timed reunitarisation period < 0");
+            c->timed_reunit = int(value);
+            return YMFLOW_OK;
         default: return fail(c, YMFLOW_ERR_ARG, "unknown option");
     }
 }
@@ -797,6 +992,8 @@ int ymflow_get_option(const ymflow_ctx* c, int key, int64_t* value) {
         case YMFLOW_OPT_OBS_BLOCK: *value = 192; return YMFLOW_OK;
         case YMFLOW_OPT_GRAPH: *value = c->use_graph ? 1 : 0; return YMFLOW_OK;
         case YMFLOW_OPT_STAGE_FORM: *value = c->stage_form; return YMFLOW_OK;
+        case YMFLOW_OPT_TILE: *value = c->tile_ok ? (int64_t(c->tile.ty) << 16) | c->tile.tz : 0; return YMFLOW_OK;
+        case YMFLOW_OPT_TIMED_REUNIT: *value = c->timed_reunit; return YMFLOW_OK;
         default: return YMFLOW_ERR_ARG;
     }
 }

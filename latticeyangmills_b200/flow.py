@@ -247,6 +247,19 @@ class GluonField:
         self._check(N.load().ymflow_get_option(self.ctx, int(key), ctypes.byref(v)))
         return v.value
 
+    def autotune(self, eps: float = 0.01):
+        """Times every stage form and tiling on this lattice and keeps the
+        fastest (cached per extents and precision); returns (form, ty, tz)."""
+        f, ty, tz = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        self._check(N.load().ymflow_autotune(self.ctx, float(eps), ctypes.byref(f), ctypes.byref(ty),
+                                             ctypes.byref(tz)))
+        return f.value, ty.value, tz.value
+
+    def set_tile(self, ty: int, tz: int) -> None:
+        """The shared-memory stage kernel's tile (form 2), and that form."""
+        self.set_option(N.OPT_TILE, (int(ty) << 16) | int(tz))
+        self.set_option(N.OPT_STAGE_FORM, N.STAGE_TILE)
+
     def device_bytes(self) -> int:
         b = ctypes.c_int64(0)
         self._check(N.load().ymflow_device_bytes(self.ctx, ctypes.byref(b)))

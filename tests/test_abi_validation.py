@@ -74,6 +74,12 @@ def test_allocation_free_entry_point_checks_before_the_device():
     assert lib.ymflow_observables_noalloc(ctypes.c_void_p(1), big, out, None) == N.ERR_CAPACITY
     bad = (ctypes.c_int * 4)(4, 0, 4, 4)
     assert lib.ymflow_observables_noalloc(ctypes.c_void_p(1), bad, out, None) == N.ERR_ARG
+    # a caller's pool offset that is not 16-byte aligned (links) or 8-byte aligned
+    # (output) is refused before anything touches a device
+    small = (ctypes.c_int * 4)(4, 4, 4, 4)
+    aligned = ctypes.c_void_p(4096)
+    assert lib.ymflow_observables_noalloc(ctypes.c_void_p(4096 + 8), small, aligned, None) == N.ERR_ARG
+    assert lib.ymflow_observables_noalloc(aligned, small, ctypes.c_void_p(4096 + 4), None) == N.ERR_ARG
 
 
 def test_valid_create_without_a_b200_says_so():

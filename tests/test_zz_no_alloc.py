@@ -29,7 +29,11 @@ def test_noalloc_observables_match_ymflow_observables_twice():
 
     lib = N.load()
     cases = [load_case("g8_metropolis"), load_case("g3456_expiah")]
-    for call, case in enumerate(cases):  # two calls in a row, different lattices
+    side = torch.cuda.Stream()
+    # two calls in a row, different lattices: the first on the default stream,
+    # the second (a smaller lattice, after the first's partials stay in the
+    # shared array) on a non-default stream
+    for call, case in enumerate(cases):
         n = tuple(case["dims"])
         U = case_field(case)
         with GluonField(n, "fp64") as f:
@@ -40,10 +44,14 @@ def test_noalloc_observables_match_ymflow_observables_twice():
         out = torch.full((4,), float("nan"), dtype=torch.float64, device="cuda")
         dims = (ctypes.c_int * 4)(*n)
         torch.cuda.synchronize()
+        stream = None if call == 0 else ctypes.c_void_p(side.cuda_stream)
         st = lib.ymflow_observables_noalloc(ctypes.c_void_p(links.data_ptr()), dims,
-                                            ctypes.c_void_p(out.data_ptr()), None)
+                                            ctypes.c_void_p(out.data_ptr()), stream)
         assert st == N.OK, (call, st)
-        torch.cuda.synchronize()
+        if call == 0:
+            torch.cuda.synchronize()
+        else:
+            side.synchronize()
         plaq, topc, energy, flag = out.cpu().numpy().tolist()
         assert flag == 0.0
         np.testing.assert_allclose(plaq, want.plaq, rtol=RTOL, atol=0)
