@@ -57,6 +57,7 @@ EPS = 0.01
 A = 0.35
 SEED = 20260
 T_CHECK = 400  # accuracy check: flow to t = 4.0 (config: eps 0.01, 400 steps)
+REUNIT_EVERY = 10  # the mixed forms' FP64 reunitarisation period (the 32^4 configuration's)
 LINK_BYTES = {"fp64": 144, "fp32_18": 72, "fp32_12": 48}
 FORCE_BYTES = {"fp64": 64, "fp32_18": 32, "fp32_12": 32}
 
@@ -85,6 +86,25 @@ def split_bytes_per_link(prec: str):
 # per 3x3 complex product, plus about 300 scalar flops (projection, RK combine,
 # tr Q^3, Cayley-Hamilton coefficients, f0 + f1 Q + f2 Q^2).
 FLOPS_PER_LINK_STAGE = 15 * 198 + 300
+
+
+STAGE_KERNELS = {
+    0: ("rk_stage", "rk_stage_kernel (fused RK3 stage, staples per link)"),
+    1: ("rk_split_stage", "rk_split_stage_kernel (RK3 stage from the stored plaquette field)"),
+    2: ("rk_tile_stage", "rk_tile_stage_kernel (one-kernel RK3 stage, a tile's plaquette field in shared memory)"),
+}
+
+
+def roofline_8d(prec: str, links: int, lups: float, stage_launch_s: float, peak_gbs: float) -> dict:
+    """The HBM roofline on the compulsory bytes of the three stages
+    (6 s_U + 4 s_Z per link-update, whatever the kernels move): `frac` for one
+    stage launch (a third of them over its duration) and `step_frac` for the
+    whole step at `lups` link-updates/s."""
+    per_launch = bytes_per_link_update(prec) * links / 3.0
+    achieved = per_launch / stage_launch_s / 1e9
+    step = lups * bytes_per_link_update(prec) / 1e9
+    return {"algorithmic_bytes_per_launch": per_launch, "achieved": achieved, "frac": achieved / peak_gbs,
+            "step_achieved": step, "step_frac": step / peak_gbs}
 
 
 def measured_peaks():
@@ -418,6 +438,7 @@ def our_arm(args, dist: Dist):
     prec = args.precision
     dev = dist.local
     seed = SEED + 1000 * dist.rank
+    reunit = 0 if prec == "fp64" else REUNIT_EVERY
 
     f = GluonField(DIMS, prec, device=dev)
     f.init_links("expiah", A, seed)
@@ -429,6 +450,11 @@ def our_arm(args, dist: Dist):
         if dist.rank == 0:
             print(json.dumps({"profile": True, "kernel": "observables", "precision": prec, "lattice": list(DIMS)}))
         return
+    # the stage form and tile: the project's autotuner (cached per lattice and precision)
+    tuned = None if args.no_autotune else f.autotune(EPS)
+    form = f.get_option(N.OPT_STAGE_FORM)
+    tile = f.get_option(N.OPT_TILE)
+    f.set_option(N.OPT_TIMED_REUNIT, reunit)  # the FP64 reunitarisation of the mixed forms, every 10 steps
     f.time_steps(EPS, args.warmup)  # untimed warm-up
 
     clocks = ClockSampler(dev)
@@ -436,60 +462,66 @@ def our_arm(args, dist: Dist):
     time.sleep(0.5)
     f.time_steps(EPS, max(args.warmup, 3))  # brings clocks up before the sampled window
     dist.barrier()
-    elapsed_ms, kernel_ms = f.time_steps(EPS, args.steps, kernels=False)
+    elapsed_ms, _ = f.time_steps(EPS, args.steps)
     dist.barrier()
     if args.profile:
         clocks.stop()
         f.close()
         if dist.rank == 0:
-            print(json.dumps({"profile": True, "precision": prec, "lattice": list(DIMS),
+            print(json.dumps({"profile": True, "precision": prec, "lattice": list(DIMS), "stage_form": form,
                               "ms_per_step": elapsed_ms / args.steps}))
         return
-    # kernel durations, measured with events around every launch of a second timed pass
-    split = f.get_option(N.OPT_STAGE_FORM) == 1
+    # The stage kernels alone, in the same graph-replayed execution without the
+    # reunitarisation (per launch: a third of a step), and with events around
+    # every launch of a third pass (instrumented: no graph).
+    f.set_option(N.OPT_TIMED_REUNIT, 0)
+    graph_ms, _ = f.time_steps(EPS, args.steps)
     _, field_ms, stage_ms = f.time_kernels(EPS, args.steps)
-    kernel_ms = field_ms + stage_ms
+    f.set_option(N.OPT_TIMED_REUNIT, reunit)
     clocks.stop()
     t_max = dist.max(elapsed_ms / 1e3)
     value = dist.world * links * args.steps / t_max
+    n_reunit = args.steps // reunit if reunit else 0
 
-    # FP64 path on the same workload (the "vs FP64" of the metric)
-    fp64_value = None
+    # FP64 path on the same workload (the "vs FP64" of the metric), autotuned the same way
+    fp64_value = fp64_form = None
     if prec != "fp64":
         g = GluonField(DIMS, "fp64", device=dev)
         g.init_links("expiah", A, seed)
+        if not args.no_autotune:
+            g.autotune(EPS)
+        fp64_form = g.get_option(N.OPT_STAGE_FORM)
         g.time_steps(EPS, args.warmup)
         dist.barrier()
         ms64, _ = g.time_steps(EPS, args.steps)
         fp64_value = dist.world * links * args.steps / dist.max(ms64 / 1e3)
         g.close()
 
-    # roofline of the dominant kernel: the stage kernel (fused, or the second
-    # kernel of the two-kernel stage); the plaquette-field kernel beside it
+    # roofline of the dominant kernel, on the compulsory bytes of the three stages
     peak, peak_kind = measured_peaks()
+    kprefix, kname = STAGE_KERNELS[form]
+    split = form == 1
+    kernels_per_stage = 2 if split else 1
+    if split:  # the stage kernel's share of the graph-timed stage, from the instrumented pass
+        stage_launch_s = graph_ms / 1e3 / (3 * args.steps) * stage_ms / (field_ms + stage_ms)
+    else:
+        stage_launch_s = graph_ms / 1e3 / (3 * args.steps)
+    roof = roofline_8d(prec, links, value / dist.world, stage_launch_s, peak)
+    alg = roof["algorithmic_bytes_per_launch"]
+    traffic = profiled_traffic(prec, DIMS, alg, kprefix)
     field_roof = None
     if split:
         field_b, stage_b = split_bytes_per_link(prec)
-        bpl = stage_b * links
-        kname = "rk_split_stage_kernel (RK3 stage from the plaquette field)"
         field_s = field_ms / 1e3 / (3 * args.steps)
-        field_ach = field_b * links / field_s / 1e9
-        field_tr = profiled_traffic(prec, DIMS, field_b * links, "plaq_field")
-        field_roof = {"kernel": "plaq_field_kernel (six plane generators per site)", "bound": "hbm",
-                      "achieved": field_ach, "peak": peak, "unit": "GB/s", "frac": field_ach / peak,
-                      "traffic": field_tr, "algorithmic_bytes_per_launch": field_b * links,
-                      "avg_launch_ms": field_s * 1e3, "share_of_kernel_time": field_ms / kernel_ms}
-    else:
-        bpl = bytes_per_link_update(prec) * links / 3.0  # algorithmic bytes per stage launch
-        kname = "rk_stage_kernel (fused RK3 stage)"
-    avg_launch_s = stage_ms / 1e3 / (3 * args.steps)
-    achieved = bpl / avg_launch_s / 1e9
-    traffic = profiled_traffic(prec, DIMS, bpl, "rk_split_stage" if split else "rk_stage")
+        field_roof = {"kernel": "plaq_field_kernel (six plane generators per site)",
+                      "design_bytes_per_launch": field_b * links, "avg_launch_ms_events": field_s * 1e3,
+                      "design_frac": field_b * links / field_s / 1e9 / peak,
+                      "share_of_kernel_time": field_ms / (field_ms + stage_ms)}
     # arithmetic roofline: the reference algorithm's flops over the step's kernel
     # time, against the measured CUDA-core FMA peak
     fma_tf = ctypes.c_double(0.0)
     N.check(N.load().ymflow_fma_peak(dev, N.FP64 if prec == "fp64" else N.FP32_18, ctypes.byref(fma_tf)))
-    alu_achieved = links * FLOPS_PER_LINK_STAGE / (kernel_ms / 1e3 / (3 * args.steps)) / 1e12
+    alu_achieved = links * FLOPS_PER_LINK_STAGE / (graph_ms / 1e3 / (3 * args.steps)) / 1e12
 
     # accuracy of the mixed form against FP64 at t = 4 (400 steps), same seeded field
     accuracy = None
@@ -498,14 +530,16 @@ def our_arm(args, dist: Dist):
         for p in sorted({prec, "fp64"}):
             h = GluonField(DIMS, p, device=dev)
             h.init_links("expiah", A, SEED)
-            rows = h.flow(EPS, T_CHECK, 0, reunit_every=10 if p != "fp64" else 0)
+            if not args.no_autotune:
+                h.autotune(EPS)  # the cached choice of the timed contexts
+            rows = h.flow(EPS, T_CHECK, 0, reunit_every=REUNIT_EVERY if p != "fp64" else 0)
             res[p] = rows[-1]
             h.close()
         r64, rm = res["fp64"], res[prec]
         accuracy = {"t": float(rm[1]), "t2E_fp64": float(r64[5]), "t2E": float(rm[5]),
                     "rel_err_t2E": abs(float(rm[5]) - float(r64[5])) / abs(float(r64[5])),
                     "Q_fp64": float(r64[3]), "abs_err_Q": abs(float(rm[3]) - float(r64[3])),
-                    "abs_err_plaq": abs(float(rm[2]) - float(r64[2])), "reunit_every": 10}
+                    "abs_err_plaq": abs(float(rm[2]) - float(r64[2])), "reunit_every": REUNIT_EVERY}
 
     # end to end through the C ABI with host buffers: upload the .bin-layout FP64
     # configuration from pinned memory, flow K steps, read the observables back
@@ -521,7 +555,7 @@ def our_arm(args, dist: Dist):
     t0 = time.perf_counter()
     for _ in range(e2e_iters):
         f.upload(hbuf)
-        rows = f.flow(EPS, args.steps, 0, reunit_every=10 if prec != "fp64" else 0)
+        rows = f.flow(EPS, args.steps, 0, reunit_every=reunit)
     t_e2e = dist.max(time.perf_counter() - t0)
     e2e_value = dist.world * links * args.steps * e2e_iters / t_e2e
     N.load().ymflow_host_free(host)
@@ -541,7 +575,7 @@ def our_arm(args, dist: Dist):
     f.close()
 
     if dist.rank == 0:
-        launches = 3 * args.steps * (2 if split else 1)
+        launches = 3 * args.steps * kernels_per_stage + n_reunit
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
@@ -551,14 +585,30 @@ def our_arm(args, dist: Dist):
             "config": {"workload": "32^4 Wilson flow, Luscher RK3, eps = 0.01",
                        "lattice": list(DIMS), "precision": prec,
                        "reductions": "f64", "l2": "inputs larger than L2 (links + generator > 126 MB)",
+                       "reunit_every": reunit or None,
+                       "timed_region": "K RK3 steps%s, graph-replayed" % (
+                           ", with the FP64 reunitarisation after every %d-th (%d launches)" % (reunit, n_reunit)
+                           if reunit else ""),
                        "parallelism": "replicas x%d" % dist.world,
-                       "fp64_link_updates_per_s": fp64_value,
+                       "stage_form": form, "tile": [tile >> 16, tile & 0xFFFF] if form == 2 else None,
+                       "autotuned": tuned is not None,
+                       "fp64_link_updates_per_s": fp64_value, "fp64_stage_form": fp64_form,
                        "mixed_over_fp64": (value / fp64_value) if fp64_value else None},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+            "roofline": {"bound": "hbm", "achieved": roof["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": roof["frac"], "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": kname,
-                         "algorithmic_bytes_per_launch": bpl,
-                         "avg_launch_ms": avg_launch_s * 1e3,
+                         "bytes": "compulsory bytes of the three stages, 6 s_U + 4 s_Z per link-update "
+                                  "(%d B), a third per stage launch" % bytes_per_link_update(prec),
+                         "algorithmic_bytes_per_launch": alg,
+                         "avg_launch_ms": stage_launch_s * 1e3,
+                         "avg_launch_ms_events": stage_ms / (3 * args.steps),
+                         "launch_time_from": "graph-replayed steps without the reunitarisation, a third of a "
+                                             "step per stage launch%s" % (
+                                                 " times the stage kernel's share of the instrumented pass"
+                                                 if split else ""),
+                         "frac_8d": roof["frac"],
+                         "step_achieved": roof["step_achieved"], "step_frac_8d": roof["step_frac"],
+                         "dram_over_compulsory": traffic / alg if traffic else None,
                          "field_kernel": field_roof},
             "alu_roofline": {"bound": "fp64 fma" if prec == "fp64" else "fp32 fma", "achieved": alu_achieved,
                              "peak": fma_tf.value, "unit": "TFLOP/s", "frac": alu_achieved / fma_tf.value,
@@ -568,7 +618,8 @@ def our_arm(args, dist: Dist):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes / args.steps,
                     "d2h_bytes_per_step": rows_bytes / args.steps,
                     "what": "per job: ymflow_upload of the .bin-layout FP64 field from pinned host memory, "
-                            "ymflow_flow of K steps, observables rows back to the host"},
+                            "ymflow_flow of K steps (reunitarisation every %s), observables rows back to the host"
+                            % (reunit or "never")},
             "ensemble": ensemble,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
@@ -669,6 +720,8 @@ def main():
                     help="with --profile: the RK stage kernels or the observables kernel")
     ap.add_argument("--decompose", action="store_true",
                     help="one 32^4 configuration split along t over the ranks (NCCL halo exchange)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default stage form instead of the autotuner's choice")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps of one precision (for ncu captures)")
     args = ap.parse_args()

@@ -1,7 +1,7 @@
 """ctypes binding of libymflow.so (the C ABI in include/ymflow.h).
 
 The library is built in-tree (latticeyangmills_b200/libymflow.so) by
-``latticeyangmills_b200.build.build()``.  There is no CPU fallback: if the
+``__graft_entry__.build()`` (or ``make -C latticeyangmills_b200/csrc``).  There is no CPU fallback: if the
 library is missing, importing the binding raises.
 """
 from __future__ import annotations
@@ -82,7 +82,8 @@ def load():
         return _lib
     if not LIB_PATH.exists():
         raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -c 'import "
-                           "latticeyangmills_b200.build as b; b.build()'` (nvcc, sm_100a)")
+                           "__graft_entry__ as g; g.build()'` from the repository root, or "
+                           "`make -C latticeyangmills_b200/csrc` (nvcc, sm_100a)")
     l = ctypes.CDLL(str(LIB_PATH))
     vp = ctypes.c_void_p
     l.ymflow_version.restype = ctypes.c_char_p

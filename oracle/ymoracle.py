@@ -27,10 +27,17 @@ _D = ctypes.POINTER(ctypes.c_double)
 _I4 = ctypes.c_int * 4
 
 
+def reference_tree():
+    """The reference's source tree: $YM_REFERENCE, else a checkout named
+    `reference` beside this repository; None where neither exists."""
+    p = Path(os.environ["YM_REFERENCE"]) if os.environ.get("YM_REFERENCE") else HERE.parent.parent / "reference"
+    return p if p.is_dir() else None
+
+
 def build() -> None:
     """Compile the oracle (and the reference harness where the reference tree exists)."""
     targets = ["oracle"]
-    if Path(os.environ.get("YM_REFERENCE", "/root/reference")).is_dir():
+    if reference_tree() is not None:
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", str(HERE)] + targets, check=True)
 

@@ -156,3 +156,22 @@ def test_bench_byte_accounting_and_profiled_traffic():
     got = bench.profiled_traffic("fp32_12", (32, 32, 32, 32), alg, "plaq_field")
     assert got == pytest.approx(372003840 / 402653184 * alg)
     assert bench.profiled_traffic("fp32_12", (16, 16, 16, 16), alg, "rk_split_stage") is None
+
+
+def test_bench_roofline_on_compulsory_bytes():
+    """bench.py's HBM fractions on the compulsory bytes of the three stages
+    (416 B per link-update for FP32-12): one stage launch carries a third of
+    them; the step fraction is link-updates/s x bytes.  The numbers of the
+    first measured line (0.2029 ms per stage launch, 4.27e9 LU/s) give the
+    kernel and step fractions 0.44 and 0.27 of 6549 GB/s."""
+    import bench
+
+    links = 4 * 32 ** 4
+    r = bench.roofline_8d("fp32_12", links, 4.27e9, 0.2029e-3, 6549.0)
+    assert r["algorithmic_bytes_per_launch"] == pytest.approx(416 / 3 * links)
+    assert r["achieved"] == pytest.approx(416 / 3 * links / 0.2029e-3 / 1e9)
+    assert r["frac"] == pytest.approx(0.4377, abs=5e-4)
+    assert r["step_achieved"] == pytest.approx(4.27e9 * 416 / 1e9)
+    assert r["step_frac"] == pytest.approx(0.2712, abs=5e-4)
+    r64 = bench.roofline_8d("fp64", links, 2.11e9, 0.5e-3, 6549.0)
+    assert r64["step_frac"] == pytest.approx(2.11e9 * 1120 / 1e9 / 6549.0)
