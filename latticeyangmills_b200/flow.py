@@ -383,6 +383,23 @@ def slab_partition(nt_global: int, nranks: int, rank: int):
     return t0, nt, (rank - 1) % nranks, (rank + 1) % nranks
 
 
+def slab_halo_plan(nt: int):
+    """The halo exchange of a time slab after every RK3 stage, in the posting
+    order of the library's NCCL exchange (csrc/slab.cu): local slices are
+    0 (lower halo), 1..nt (interior), nt + 1 (upper halo).  Each entry: the
+    interior slice this rank sends and the neighbour it goes to, and the halo
+    slice it receives and the neighbour that sends it.  A send of one entry
+    lands in the receive of the same entry on the other side; `tag` numbers
+    the entries, so that a rank that is the neighbour on both sides (two
+    ranks) or its own neighbour (one) tells the two transfers apart.  It replaces shift()'s face exchange (include/Math/lattice.h:437-449)."""
+    if nt < 1:
+        raise ValueError("a slab holds at least one time slice")
+    return [
+        {"send_slice": 1, "to": "lower", "recv_slice": nt + 1, "from": "upper", "tag": 0},
+        {"send_slice": nt, "to": "upper", "recv_slice": 0, "from": "lower", "tag": 1},
+    ]
+
+
 def slab_group_flow(slabs: Sequence[GluonField], eps: float, nsteps: int, measure_every: int = 1,
                     reunit_every: int = 0) -> np.ndarray:
     """ymflow_flow over the slabs of one configuration held in this process

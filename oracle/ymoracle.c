@@ -258,6 +258,23 @@ void yo_flow_step(double* U, double* Z, const int n[4], double eps) {
     update_links(U, Z, V, eps, 1.0, 0);                     /* W3 (:169-171) */
 }
 
+/* One of the three stages of yo_flow_step alone (stage 0, 1, 2): the pieces of
+ * src/Apps/wilsonflow.cpp:143-149, :152-160 and :163-171.  Lets a caller run
+ * a decomposed lattice stage by stage with its halos exchanged in between. */
+void yo_flow_stage(double* U, double* Z, const int n[4], double eps, int stage) {
+    long V = volume(n);
+    if (stage == 0) {
+        combine_force(U, Z, n, 0.0, 0.0, 1);
+        update_links(U, Z, V, eps, 1.0 / 4.0, 1);
+    } else if (stage == 1) {
+        combine_force(U, Z, n, 8.0 / 9.0, 17.0 / 36.0, 0);
+        update_links(U, Z, V, eps, 1.0, 0);
+    } else {
+        combine_force(U, Z, n, 3.0 / 4.0, 1.0, 0);
+        update_links(U, Z, V, eps, 1.0, 0);
+    }
+}
+
 /* ---------------------------------------------------------------------------
  * Observables (src/Observables/superobs.cpp:31-128)
  * ------------------------------------------------------------------------- */

@@ -29,6 +29,7 @@ void yo_exp_many(const double* q, double* r, long n);
 void yo_derivative(const double* U, const int n[4], int mu, double* Zmu);
 /* One Luscher RK3 step in place (src/Apps/wilsonflow.cpp:141-172).  Z: V x 4 x 18 scratch. */
 void yo_flow_step(double* U, double* Z, const int n[4], double eps);
+void yo_flow_stage(double* U, double* Z, const int n[4], double eps, int stage);
 /* plaq, topc, energy exactly as SuperObs::compute (src/Observables/superobs.cpp:31-128). */
 void yo_superobs(const double* U, const int n[4], double out[3]);
 /* nsteps RK3 steps; rows (step, t, plaq, topc, energy) at step 0 and every `every` steps

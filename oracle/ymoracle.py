@@ -54,6 +54,7 @@ def lib():
         l.yo_exp_many.argtypes = [_D, _D, ctypes.c_long]
         l.yo_derivative.argtypes = [_D, _I4, ctypes.c_int, _D]
         l.yo_flow_step.argtypes = [_D, _D, _I4, ctypes.c_double]
+        l.yo_flow_stage.argtypes = [_D, _D, _I4, ctypes.c_double, ctypes.c_int]
         l.yo_superobs.argtypes = [_D, _I4, _D]
         l.yo_flow.argtypes = [_D, _I4, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D]
         l.yo_flow.restype = ctypes.c_int
@@ -139,6 +140,12 @@ def superobs(U: np.ndarray, n):
     o = np.zeros(3)
     lib().yo_superobs(_p(U), _dims(n), _p(o))
     return float(o[0]), float(o[1]), float(o[2])
+
+
+def flow_stage(U: np.ndarray, Z: np.ndarray, n, eps: float, stage: int) -> None:
+    """One RK3 stage (0, 1, 2) of U in place on the periodic lattice n; Z (4 V
+    x 18 doubles) carries the RK generator between the stages of a step."""
+    lib().yo_flow_stage(_p(U), _p(Z), _dims(n), eps, int(stage))
 
 
 def flow(U: np.ndarray, n, eps: float, nsteps: int, every: int) -> np.ndarray:

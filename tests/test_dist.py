@@ -88,3 +88,93 @@ def test_decomposed_mode_host_logic_on_three_ranks():
     assert all(r[2] == parts for r in res)
     assert [p[0] for p in parts] == [0, 11, 22] and [p[1] for p in parts] == [11, 11, 10]
     assert [(p[2], p[3]) for p in parts] == [(2, 1), (0, 2), (1, 0)]
+
+
+# --- the halo data path on CPU ranks ------------------------------------------------
+# Each gloo rank holds one time slab of a configuration (its slices plus one
+# halo slice on each side), flows it with the CPU oracle one RK3 stage at a
+# time, and after every stage exchanges halo slices with its neighbours on the
+# library's schedule (slab_halo_plan).  Gathered, the interiors must equal the
+# whole-lattice oracle flow link for link: the exchange carries exactly the
+# faces the stages need.
+FLOW_N = (4, 3, 2, 7)  # x, y, z, t: 7 time slices over 2 or 3 ranks, uneven slabs
+FLOW_STEPS, FLOW_EPS = 3, 0.02
+
+
+def _flow_rank_main(rank, world, port, q):
+    import sys
+
+    import numpy as np
+
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch
+    import torch.distributed as dist
+
+    from latticeyangmills_b200 import slab_halo_plan, slab_partition
+    from oracle import ymoracle as yo
+
+    dist.init_process_group("gloo")
+    n = FLOW_N
+    t0, nt, lower, upper = slab_partition(n[3], world, rank)
+    whole = yo.gen_expiah(n, 0.4, 11)  # (t, z, y, x, 4, 18)
+    local = np.ascontiguousarray(np.concatenate([whole[(t0 - 1) % n[3]][None], whole[t0:t0 + nt],
+                                                 whole[(t0 + nt) % n[3]][None]]))
+    ln = (n[0], n[1], n[2], nt + 2)
+    Z = np.zeros_like(local)
+    peer = {"lower": lower, "upper": upper}
+    for _ in range(FLOW_STEPS):
+        for stage in range(3):
+            yo.flow_stage(local, Z, ln, FLOW_EPS, stage)  # interior slices exact, halos stale
+            reqs, bufs = [], []
+            for tr in slab_halo_plan(nt):
+                reqs.append(dist.isend(torch.from_numpy(local[tr["send_slice"]].copy()), peer[tr["to"]],
+                                       tag=tr["tag"]))
+                buf = torch.empty(local[0].shape, dtype=torch.float64)
+                # the neighbour's send of the same plan entry lands here
+                reqs.append(dist.irecv(buf, peer[tr["from"]], tag=tr["tag"]))
+                bufs.append((tr["recv_slice"], buf))
+            for r in reqs:
+                r.wait()
+            for sl, buf in bufs:
+                local[sl] = buf.numpy()
+    parts = [None] * world
+    dist.all_gather_object(parts, (t0, local[1:nt + 1].copy()))
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        got = np.concatenate([p[1] for p in sorted(parts, key=lambda p: p[0])])
+        want = whole.copy()
+        for _ in range(FLOW_STEPS):
+            yo.flow(want, n, FLOW_EPS, 1, 0)
+        q.put(float(np.abs(got - want).max()))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_halo_exchange_reproduces_the_whole_lattice_flow(world):
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_flow_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    assert q.get(timeout=10) == 0.0  # bit for bit
+
+
+def test_halo_plan_pairs_every_send_with_a_receive():
+    from latticeyangmills_b200 import slab_halo_plan
+
+    for nt in (1, 2, 5):
+        plan = slab_halo_plan(nt)
+        assert [(tr["send_slice"], tr["to"]) for tr in plan] == [(1, "lower"), (nt, "upper")]
+        assert [(tr["recv_slice"], tr["from"]) for tr in plan] == [(nt + 1, "upper"), (0, "lower")]
+        # what a rank sends down arrives in its lower neighbour's upper halo, and back
+        assert {tr["to"]: tr["tag"] for tr in plan} == {"lower": 0, "upper": 1}
+    with pytest.raises(ValueError):
+        slab_halo_plan(0)
