@@ -352,11 +352,28 @@ YMFLOW_API int ymflow_ensemble_flow(ymflow_ens* ens, double eps, int nsteps, int
 YMFLOW_API int ymflow_ensemble_reset_time(ymflow_ens* ens);
 /* Device-timed RK3 steps of the whole ensemble (no measurements). */
 YMFLOW_API int ymflow_ensemble_time_steps(ymflow_ens* ens, double eps, int nsteps, float* elapsed_ms);
-/* Times the stage kernel over persistent grids {one CTA per work item, 1x and
- * 2x the resident CTAs} (128 threads per block), keeps the fastest, and
- * caches it for every ensemble of the same sizes and precision in the process.
+/* The project's autotuner for an ensemble: times one RK3 stage of the whole
+ * ensemble in each form it can take and keeps the fastest, cached for every
+ * ensemble of the same sizes and precision in the process:
+ *   - the per-link kernel (FP64) over persistent grids {one CTA per work
+ *     item, 1x and 2x the resident CTAs}, or the two-kernel stage (FP32), one
+ *     block per 32-site item;
+ *   - the one-kernel stage with tiles in shared memory (YMFLOW_OPT_STAGE_FORM
+ *     2 of a single context) at 128, 256, 384 or 512 threads per block: every
+ *     configuration gets the tile of at most that many sites (whole x lines,
+ *     a ty x tz patch of (y, z)) with the least estimated time per site, and
+ *     one persistent launch per stage streams along t through the tile units
+ *     of all configurations.
+ * Writes the block size and grid of the choice (grid 0: one block per item).
  * Does not change the flow state. */
 YMFLOW_API int ymflow_ensemble_autotune(ymflow_ens* ens, double eps, int* block, int* grid);
+/* The ensemble's current stage form (0 per-link kernel, 1 two-kernel stage,
+ * 2 tiles in shared memory), block size and grid. */
+YMFLOW_API int ymflow_ensemble_tuning(const ymflow_ens* ens, int* stage_form, int* block, int* grid);
+/* Sets the form by hand: 0 with block 128 and a grid (0: one block per item),
+ * 1 (FP32 ensembles) with block 128, or 2 with `block` threads (grid chosen
+ * from the occupancy).  YMFLOW_ERR_ARG where the form cannot run. */
+YMFLOW_API int ymflow_ensemble_set_tuning(ymflow_ens* ens, int stage_form, int block, int grid);
 
 #ifdef __cplusplus
 }

@@ -44,7 +44,7 @@ EXPORTS = (
     "ymflow_ensemble_create", "ymflow_ensemble_destroy", "ymflow_ensemble_last_error",
     "ymflow_ensemble_upload", "ymflow_ensemble_download", "ymflow_ensemble_init_links",
     "ymflow_ensemble_flow", "ymflow_ensemble_reset_time", "ymflow_ensemble_time_steps",
-    "ymflow_ensemble_autotune", "ymflow_observables_noalloc",
+    "ymflow_ensemble_autotune", "ymflow_ensemble_tuning", "ymflow_ensemble_set_tuning", "ymflow_observables_noalloc",
     "ymflow_create_slab", "ymflow_nccl_unique_id", "ymflow_slab_connect", "ymflow_slab_group_flow",
 )
 NON_INT = ("ymflow_version", "ymflow_create", "ymflow_create_slab", "ymflow_destroy", "ymflow_last_error",
@@ -138,6 +138,8 @@ def load():
     l.ymflow_ensemble_reset_time.argtypes = [vp]
     l.ymflow_ensemble_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     l.ymflow_ensemble_autotune.argtypes = [vp, ctypes.c_double, IP, IP]
+    l.ymflow_ensemble_tuning.argtypes = [vp, IP, IP, IP]
+    l.ymflow_ensemble_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     l.ymflow_observables_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_int), vp, vp]
     l.ymflow_create_slab.argtypes = [IP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, IP]
     l.ymflow_create_slab.restype = vp

@@ -18,8 +18,7 @@
 #include <vector>
 
 #include "api_util.h"
-#include "flow_device.cuh"
-#include "kernels.h"
+#include "flow_tile.cuh"
 #include "ymflow.h"
 
 namespace ym {
@@ -31,6 +30,8 @@ struct EnsConf {
     int64_t hoff;  // start in the plane-generator pool of the two-kernel stage (bytes, 16-aligned)
     int blk0;      // first work item
     int nblk;      // work items (blocks of sites)
+    TileShape tp;  // the tile kernel's tiling of this configuration
+    int unit0;     // its first tile unit in the ensemble's unit list
 };
 
 __device__ __forceinline__ int find_conf(const EnsConf* confs, int nconf, int item) {
@@ -163,6 +164,114 @@ static cudaError_t launch_ens_split_typed(int stage, void* uin, void* uout, void
     return cudaGetLastError();
 }
 
+// The one-kernel stage with a tile's plaquette field in shared memory
+// (flow_tile.cuh) over every configuration at once: the unit lists of all
+// configurations, concatenated, are split into contiguous runs, one per
+// persistent block; a block streams through its run along t, crossing from
+// one tile column or configuration to the next.  Every configuration's tile
+// has at most blockDim.x sites (threads beyond a tile's sites only help with
+// its plane generators).
+__device__ __forceinline__ int find_unit_conf(const EnsConf* confs, int nconf, int unit) {
+    int lo = 0, hi = nconf - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&confs[mid].unit0) <= unit) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class F, int STAGE>
+__global__ void __launch_bounds__(512, 1)
+    ens_tile_kernel(char* uin, char* uout, char* z, const EnsConf* __restrict__ confs, int nconf, int nunits,
+                    typename F::Real eps) {
+    using R = typename F::Real;
+    using V = typename HVec<R>::V;
+    extern __shared__ __align__(16) unsigned char ens_tile_smem[];
+    V* const sm = reinterpret_cast<V*>(ens_tile_smem);
+    const int u0 = int((long long)blockIdx.x * nunits / gridDim.x);
+    const int u1 = int((long long)(blockIdx.x + 1) * nunits / gridDim.x);
+    int cur = 0;
+    for (int u = u0; u < u1; u++) {
+        const EnsConf& C = confs[find_unit_conf(confs, nconf, u)];
+        const int Lt = C.g.n[3];
+        const int local = u - C.unit0;
+        const int col = local / Lt, t = local - col * Lt;
+        const F in{uin + C.uoff, C.g.V}, out{uout + C.uoff, C.g.V};
+        const ForceField<R> zf{z + C.zoff, C.g.V};
+        tile_unit<F, STAGE>(in, out, zf, C.g, C.tp, eps, sm, int(threadIdx.x), int(blockDim.x), col, t,
+                            u == u0 || t == 0, cur);
+        cur ^= 1;
+    }
+}
+
+template <class F>
+static void* ens_tile_ptr(int stage) {
+    switch (stage) {
+        case 0: return (void*)ens_tile_kernel<F, 0>;
+        case 1: return (void*)ens_tile_kernel<F, 1>;
+        default: return (void*)ens_tile_kernel<F, 2>;
+    }
+}
+
+static void* ens_tile_fn(int prec, int stage) {
+    switch (prec) {
+        case kFP64: return ens_tile_ptr<FieldD18>(stage);
+        case kFP32_18: return ens_tile_ptr<FieldF18>(stage);
+        default: return ens_tile_ptr<FieldF12>(stage);
+    }
+}
+
+cudaError_t prepare_ens_tile(int prec) {
+    for (int s = 0; s < 3; s++) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(ens_tile_fn(prec, s), cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int ens_tile_resident(int prec, int threads, size_t smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_tile_fn(prec, 1), threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+template <class F>
+static cudaError_t launch_ens_tile_typed(int stage, void* uin, void* uout, void* z, const EnsConf* confs, int nconf,
+                                         int nunits, int grid, int threads, size_t smem, double eps, cudaStream_t st) {
+    using R = typename F::Real;
+    const R e = R(stage == 0 ? eps * 0.25 : eps);
+    char *a = (char*)uin, *b = (char*)uout, *zz = (char*)z;
+    switch (stage) {
+        case 0: ens_tile_kernel<F, 0><<<grid, threads, smem, st>>>(a, b, zz, confs, nconf, nunits, e); break;
+        case 1: ens_tile_kernel<F, 1><<<grid, threads, smem, st>>>(a, b, zz, confs, nconf, nunits, e); break;
+        default: ens_tile_kernel<F, 2><<<grid, threads, smem, st>>>(a, b, zz, confs, nconf, nunits, e); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ens_tile_stage(int prec, int stage, void* uin, void* uout, void* z, const EnsConf* confs,
+                                  int nconf, int nunits, int grid, int threads, size_t smem, double eps,
+                                  cudaStream_t st) {
+    if (grid < 1 || threads < 32 || threads > 512) return cudaErrorInvalidValue;
+    switch (prec) {
+        case kFP64:
+            return launch_ens_tile_typed<FieldD18>(stage, uin, uout, z, confs, nconf, nunits, grid, threads, smem,
+                                                   eps, st);
+        case kFP32_18:
+            return launch_ens_tile_typed<FieldF18>(stage, uin, uout, z, confs, nconf, nunits, grid, threads, smem,
+                                                   eps, st);
+        case kFP32_12:
+            return launch_ens_tile_typed<FieldF12>(stage, uin, uout, z, confs, nconf, nunits, grid, threads, smem,
+                                                   eps, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 // Work items must be 32-site groups (block 128).
 cudaError_t launch_ens_split_stage(int prec, int stage, void* uin, void* uout, void* z, void* h, const EnsConf* confs,
                                    int nconf, int nitems, double eps, cudaStream_t st) {
@@ -200,8 +309,11 @@ int ens_max_resident(int prec, int block) {
 }
 
 // Tuning results shared by every ensemble with the same signature in this process.
+struct EnsTuning {
+    int form, block, grid;
+};
 std::mutex g_tune_mu;
-std::map<std::string, std::pair<int, int>> g_tune_cache;
+std::map<std::string, EnsTuning> g_tune_cache;
 
 }  // namespace ym
 
@@ -219,6 +331,11 @@ struct ymflow_ens {
     void* z = nullptr;
     void* h = nullptr;       // plane generators of the two-kernel stage (FP32 ensembles)
     bool split = false;      // FP32: the two-kernel stage, one block per work item
+    bool tile = false;       // the one-kernel stage with tiles in shared memory (over split / fused)
+    int tile_threads = 0;    // its block size: every configuration's tile has at most this many sites
+    int tile_grid = 0;       // its persistent blocks
+    size_t tile_smem = 0;    // its shared memory per block (the largest configuration's)
+    int nunits = 0;          // tile units of all configurations
     int64_t pool_links = 0;  // bytes per link pool
     int64_t pool_force = 0;  // bytes of the generator pool
     double* staging = nullptr;  // .bin-layout buffer sized for the largest configuration
@@ -277,6 +394,58 @@ int set_block(ymflow_ens* e, int block) {
     return YMFLOW_OK;
 }
 
+// Tiles for every configuration with at most `threads` sites each: per
+// configuration the tile with the least estimated time per site (threads
+// idle beyond the tile's sites, recomputed faces), then the unit list and
+// the persistent grid.  false if a configuration has no such tile or the
+// largest shared memory does not fit.
+bool set_tiles(ymflow_ens* e, int threads) {
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    std::vector<TileShape> tps(e->nconf);
+    size_t smem = 0;
+    for (int c = 0; c < e->nconf; c++) {
+        const Geo& g = e->confs[c].g;
+        bool found = false;
+        double best = 0.0;
+        for (int ty = 1; ty <= g.n[1]; ty++)
+            for (int tz = 1; tz <= g.n[2]; tz++) {
+                TileShape tp;
+                if (!make_tile_shape(e->prec, g, ty, tz, &tp, false) || tp.ns > threads) continue;
+                const double cost = double(threads) / tp.ns * (12.0 + 3.0 * (tp.nfy + tp.nfz) / tp.ns);
+                if (!found || cost < best) {
+                    tps[c] = tp;
+                    best = cost;
+                    found = true;
+                }
+            }
+        if (!found) return false;
+        smem = std::max(smem, tile_smem_bytes(e->prec, tps[c]));
+    }
+    const int resident = ens_tile_resident(e->prec, threads, smem);
+    if (resident < 1) return false;
+    int unit = 0;
+    for (int c = 0; c < e->nconf; c++) {
+        e->confs[c].tp = tps[c];
+        e->confs[c].unit0 = unit;
+        unit += tps[c].units;
+    }
+    if (cudaMemcpyAsync(e->confs_dev, e->confs.data(), sizeof(EnsConf) * e->confs.size(), cudaMemcpyHostToDevice,
+                        e->stream) != cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    e->nunits = unit;
+    e->tile_threads = threads;
+    e->tile_smem = smem;
+    e->tile_grid = std::min(unit, resident * sms);
+    return true;
+}
+
 int nitems(const ymflow_ens* e) {
     return e->confs.empty() ? 0 : e->confs.back().blk0 + e->confs.back().nblk;
 }
@@ -289,10 +458,13 @@ cudaError_t enqueue_ens_step(ymflow_ens* e, int from, double eps) {
     const int ni = nitems(e);
     const int grid = e->grid > 0 ? std::min(e->grid, ni) : ni;
     for (int s = 0; s < 3; s++) {
-        cudaError_t r = e->split ? launch_ens_split_stage(e->prec, s, in[s], out[s], e->z, e->h, e->confs_dev,
-                                                          e->nconf, ni, eps, e->stream)
-                                 : launch_ens_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf, ni, grid,
-                                                    e->block, eps, e->stream);
+        cudaError_t r = e->tile ? launch_ens_tile_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf,
+                                                        e->nunits, e->tile_grid, e->tile_threads, e->tile_smem, eps,
+                                                        e->stream)
+                        : e->split ? launch_ens_split_stage(e->prec, s, in[s], out[s], e->z, e->h, e->confs_dev,
+                                                            e->nconf, ni, eps, e->stream)
+                                   : launch_ens_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf, ni,
+                                                      grid, e->block, eps, e->stream);
         if (r != cudaSuccess) return r;
     }
     return cudaSuccess;
@@ -381,12 +553,20 @@ float time_stage0(ymflow_ens* e, double eps, int reps) {
     // overwrites anyway, so tuning does not disturb the flow state
     const int ni = nitems(e);
     const int grid = e->grid > 0 ? std::min(e->grid, ni) : ni;
-    launch_ens_stage(e->prec, 0, e->u[e->cur], e->u[1 - e->cur], e->z, e->confs_dev, e->nconf, ni, grid, e->block,
-                     eps, e->stream);
+    void* a = e->u[e->cur];
+    void* b = e->u[1 - e->cur];
+    auto launch = [&]() {
+        if (e->tile)
+            return launch_ens_tile_stage(e->prec, 0, a, b, e->z, e->confs_dev, e->nconf, e->nunits, e->tile_grid,
+                                         e->tile_threads, e->tile_smem, eps, e->stream);
+        if (e->split)
+            return launch_ens_split_stage(e->prec, 0, a, b, e->z, e->h, e->confs_dev, e->nconf, ni, eps, e->stream);
+        return launch_ens_stage(e->prec, 0, a, b, e->z, e->confs_dev, e->nconf, ni, grid, e->block, eps, e->stream);
+    };
+    if (launch() != cudaSuccess) return -1.f;
     cudaEventRecord(e->ev0, e->stream);
     for (int i = 0; i < reps; i++)
-        launch_ens_stage(e->prec, 0, e->u[e->cur], e->u[1 - e->cur], e->z, e->confs_dev, e->nconf, ni, grid,
-                         e->block, eps, e->stream);
+        if (launch() != cudaSuccess) return -1.f;
     cudaEventRecord(e->ev1, e->stream);
     if (cudaEventSynchronize(e->ev1) != cudaSuccess) return -1.f;
     float ms = 0.f;
@@ -479,12 +659,21 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
     if (r == YMFLOW_OK && (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess))
         r = YMFLOW_ERR_CUDA;
     if (r == YMFLOW_OK) r = set_block(e, 128);
+    if (r == YMFLOW_OK && prepare_ens_tile(e->prec) != cudaSuccess) {
+        const cudaError_t ce = cudaGetLastError();
+        r = ecuda(e, ce == cudaSuccess ? cudaErrorInvalidValue : ce, "tile kernel set-up");
+    }
     if (r == YMFLOW_OK) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(e->signature);
         if (it != g_tune_cache.end()) {
-            e->grid = it->second.second;
-            r = set_block(e, it->second.first);
+            const EnsTuning tn = it->second;
+            if (tn.form == 2 && set_tiles(e, tn.block)) {
+                e->tile = true;
+            } else {
+                e->grid = tn.form == 2 ? 0 : tn.grid;
+                r = set_block(e, tn.form == 2 ? 128 : tn.block);
+            }
             e->tuned = true;
         }
     }
@@ -660,46 +849,89 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     for (int c = 0; c < e->nconf; c++)
         if (!e->loaded[c]) return efail(e, YMFLOW_ERR_STATE, "configuration not loaded");
     DeviceGuard guard(e->device);
-    if (e->split) {  // the two-kernel stage runs one block per 32-site item: nothing to tune
-        int r = set_block(e, 128);
-        if (r != YMFLOW_OK) return r;
-        e->grid = 0;
-        drop_graphs(e);
-        e->tuned = true;
-        if (block_out) *block_out = 128;
-        if (grid_out) *grid_out = 0;
-        return YMFLOW_OK;
-    }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+    // candidates: the per-link kernel over {one block per item, 1x and 2x the
+    // resident blocks} (FP64) or the two-kernel stage (FP32), and the tile
+    // kernel with 128 / 256 / 384 / 512 threads (tiles of at most that many sites)
+    std::vector<EnsTuning> cands;
+    if (e->split) {
+        cands.push_back({1, 128, 0});
+    } else {
+        const int resident = ens_max_resident(e->prec, 128);
+        for (int grid : {0, resident * sms, 2 * resident * sms}) cands.push_back({0, 128, grid});
+    }
+    for (int threads : {128, 256, 384, 512}) cands.push_back({2, threads, 0});
+    const bool was_split = e->split;
     float best = 1e30f;
-    int best_block = e->block, best_grid = e->grid;
-    for (int block : {128}) {
-        int r = set_block(e, block);
-        if (r != YMFLOW_OK) return r;
-        const int resident = ens_max_resident(e->prec, block);
-        for (int grid : {0, resident * sms, 2 * resident * sms}) {
-            e->grid = grid;
-            const float ms = time_stage0(e, eps, 3);
-            if (ms < 0.f) return ecuda(e, cudaGetLastError(), "tuning launch");
-            if (ms < best) {
-                best = ms;
-                best_block = block;
-                best_grid = grid;
-            }
+    EnsTuning pick = cands.front();
+    for (const EnsTuning& ch : cands) {
+        e->tile = false;
+        if (ch.form == 2) {
+            if (!set_tiles(e, ch.block)) continue;
+            e->tile = true;
+        } else {
+            e->grid = ch.grid;
+            int r = set_block(e, ch.block);
+            if (r != YMFLOW_OK) return r;
+        }
+        const float ms = time_stage0(e, eps, 3);
+        if (ms < 0.f) return ecuda(e, cudaGetLastError(), "tuning launch");
+        if (ms < best) {
+            best = ms;
+            pick = ch;
         }
     }
-    e->grid = best_grid;
-    int r = set_block(e, best_block);
-    if (r != YMFLOW_OK) return r;
+    e->tile = false;
+    e->split = was_split;
+    if (pick.form == 2 && set_tiles(e, pick.block)) {
+        e->tile = true;
+    } else {
+        e->grid = pick.form == 2 ? 0 : pick.grid;
+        int r = set_block(e, pick.form == 2 ? 128 : pick.block);
+        if (r != YMFLOW_OK) return r;
+    }
     drop_graphs(e);
     e->tuned = true;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tune_cache[e->signature] = {best_block, best_grid};
+        g_tune_cache[e->signature] = pick;
     }
-    if (block_out) *block_out = best_block;
-    if (grid_out) *grid_out = best_grid;
+    if (block_out) *block_out = e->tile ? e->tile_threads : e->block;
+    if (grid_out) *grid_out = e->tile ? e->tile_grid : e->grid;
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_set_tuning(ymflow_ens* e, int stage_form, int block, int grid) {
+    if (!e) return YMFLOW_ERR_ARG;
+    DeviceGuard guard(e->device);
+    if (stage_form == 2) {
+        if (block < 32 || block > 512 || !set_tiles(e, block))
+            return efail(e, YMFLOW_ERR_ARG, "no tiling of every configuration within " + std::to_string(block) +
+                                                " threads and 227 KB of shared memory");
+        e->tile = true;
+    } else if (stage_form == 0 || (stage_form == 1 && e->h)) {
+        if (stage_form == 1 && block != 128) return efail(e, YMFLOW_ERR_ARG, "the two-kernel stage runs 128 threads");
+        if (block != 128) return efail(e, YMFLOW_ERR_ARG, "the per-link kernel runs 128 threads");
+        if (grid < 0) return efail(e, YMFLOW_ERR_ARG, "grid < 0");
+        e->tile = false;
+        e->split = stage_form == 1;
+        e->grid = stage_form == 1 ? 0 : grid;
+        const int r = set_block(e, 128);
+        if (r != YMFLOW_OK) return r;
+    } else {
+        return efail(e, YMFLOW_ERR_ARG, "stage form is 0, 1 (FP32 ensembles) or 2");
+    }
+    YE_CK(e, cudaStreamSynchronize(e->stream), "set tuning");
+    drop_graphs(e);
+    return YMFLOW_OK;
+}
+
+int ymflow_ensemble_tuning(const ymflow_ens* e, int* stage_form, int* block, int* grid) {
+    if (!e) return YMFLOW_ERR_ARG;
+    if (stage_form) *stage_form = e->tile ? 2 : (e->split ? 1 : 0);
+    if (block) *block = e->tile ? e->tile_threads : e->block;
+    if (grid) *grid = e->tile ? e->tile_grid : e->grid;
     return YMFLOW_OK;
 }
 

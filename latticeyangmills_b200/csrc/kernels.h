@@ -53,7 +53,9 @@ struct TileShape {
 };
 // Whether (ty, tz) tiles the whole-lattice geometry g (whole warps per x-y run,
 // 64..512 threads, shared memory within 227 KB); fills *out (grid left 0).
-bool make_tile_shape(int prec, const Geo& g, int ty, int tz, TileShape* out);
+// whole_warps = false drops the warp rule (x-y runs of any length, 32..512
+// threads): correct, with warps straddling rows (the ensemble's 12^4).
+bool make_tile_shape(int prec, const Geo& g, int ty, int tz, TileShape* out, bool whole_warps = true);
 size_t tile_smem_bytes(int prec, const TileShape& tp);
 // Opt the tile kernels of a precision into their shared memory (per device).
 cudaError_t prepare_tile_kernels(int prec);

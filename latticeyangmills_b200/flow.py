@@ -343,6 +343,16 @@ class Ensemble:
         self._check(N.load().ymflow_ensemble_autotune(self._ens, float(eps), ctypes.byref(b), ctypes.byref(g)))
         return b.value, g.value
 
+    def set_tuning(self, stage_form: int, block: int = 128, grid: int = 0) -> None:
+        """Chooses the stage form by hand (see ymflow_ensemble_set_tuning)."""
+        self._check(N.load().ymflow_ensemble_set_tuning(self._ens, int(stage_form), int(block), int(grid)))
+
+    def tuning(self):
+        """(stage form, block, grid) the ensemble flows with."""
+        f, b, g = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        self._check(N.load().ymflow_ensemble_tuning(self._ens, ctypes.byref(f), ctypes.byref(b), ctypes.byref(g)))
+        return f.value, b.value, g.value
+
     def reset_time(self) -> None:
         self._check(N.load().ymflow_ensemble_reset_time(self._ens))
 

@@ -49,7 +49,9 @@ def test_autotune_keeps_state_and_results(oracle):
             a.init_links(c, "expiah", 0.35, 10 + c)
             b.init_links(c, "expiah", 0.35, 10 + c)
         block, grid = a.autotune()
-        assert block == 128 and grid >= 0
+        assert block in (128, 256, 384, 512) and grid >= 0
+        assert b.autotune() == (block, grid)  # the cached choice
+        assert a.tuning() == b.tuning()
         ra = a.flow(0.01, 4, 2)
         rb = b.flow(0.01, 4, 2)
         np.testing.assert_array_equal(ra, rb)
@@ -75,3 +77,42 @@ def test_ensemble_matches_reference_golden():
         ref = np.array(c["rows"])[:6]
         np.testing.assert_allclose(rows[:, i, 2], ref[:, 2], rtol=1e-12)
         np.testing.assert_allclose(rows[:, i, 4], ref[:, 4], rtol=1e-12)
+
+
+# lattices the tile kernel covers, 12^4 with x-y runs that straddle warps
+TILE_SIZES = [(8, 8, 8, 8), (16, 4, 4, 6), (32, 4, 6, 5), (12, 12, 12, 12)]
+
+
+@pytest.mark.parametrize("prec,threads", [("fp64", 128), ("fp64", 256), ("fp32_12", 256), ("fp32_18", 512)])
+def test_tile_ensemble_equals_one_by_one(prec, threads):
+    """The one-kernel stage with tiles in shared memory over every
+    configuration in one launch (block runs crossing configurations) against
+    each configuration on its own: FP64 link by link to 1e-13."""
+    from latticeyangmills_b200 import Ensemble
+
+    steps, every = 5, 5
+    with Ensemble(TILE_SIZES, prec) as ens:
+        ens.set_tuning(2, threads)
+        assert ens.tuning()[:2] == (2, threads)
+        for c, n in enumerate(TILE_SIZES):
+            ens.init_links(c, "expiah", 0.3 + 0.02 * c, c)
+        rows = ens.flow(0.01, steps, every, reunit_every=0)
+        for c, n in enumerate(TILE_SIZES):
+            want_rows, want_links = single(n, prec, c, steps, every)
+            assert np.abs(ens.download(c) - want_links).max() < LINK_TOL[prec]
+            np.testing.assert_allclose(rows[:, c, [2, 4]], want_rows[:, [2, 4]], rtol=OBS_RTOL[prec])
+
+
+def test_set_tuning_refusals():
+    from latticeyangmills_b200 import Ensemble, YmflowError
+
+    with Ensemble([(2, 3, 2, 4), (8, 8, 8, 8)], "fp32_12") as ens:  # 2x3x2: fewer than 32 sites a slice
+        with pytest.raises(YmflowError):
+            ens.set_tuning(2, 256)
+        with pytest.raises(YmflowError):
+            ens.set_tuning(1, 256)
+        ens.set_tuning(1)
+        assert ens.tuning()[0] == 1
+    with Ensemble([(8, 8, 8, 8)], "fp64") as ens:
+        with pytest.raises(YmflowError):
+            ens.set_tuning(1)  # no plane-generator pool in FP64 ensembles
