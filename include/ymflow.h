@@ -210,15 +210,17 @@ YMFLOW_API int ymflow_time_kernels(ymflow_ctx* ctx, double eps, int nsteps, floa
  *   0 = one fused kernel, staples summed per link (the FP64 default);
  *   1 = two kernels, the six plaquettes' generators of every site into a
  *       stored field (6 x 8 reals per site of device memory), then each link's
- *       force from them (FP32 default where form 2 has no tiling, and slabs);
+ *       force from them (the FP32 default);
  *   2 = one kernel: blocks of Lx x ty x tz sites of a time slice compute their
  *       plaquette generators into shared memory, recompute the lower (y, z)
- *       faces, stream along t and finish the links from there (the FP32
- *       default where the lattice tiles into at least one block per SM;
- *       whole-lattice contexts only).
- * YMFLOW_OPT_TILE: form 2's tile, value = (ty << 16) | tz; ty must divide the
- * y extent, tz the z extent, Lx ty must be a multiple of 32 and Lx ty tz within
- * 64..512 (YMFLOW_ERR_ARG otherwise).  YMFLOW_OPT_TIMED_REUNIT: the FP64
+ *       faces, stream along t and finish the links from there (whole-lattice
+ *       contexts only; ymflow_autotune times it against the others).
+ * YMFLOW_OPT_TILE: form 2's tiling, value = (lean << 36) | (lpt << 32) |
+ * (ty << 16) | tz: ty must divide the y extent, tz the z extent, Lx ty must be
+ * a multiple of 32 and Lx ty tz within 64..512 sites; each thread advances
+ * lpt = 1, 2 or 4 links (0 reads as 4), so a block has 4 Lx ty tz / lpt
+ * threads; lean = 1 runs the kernel compiled for 64 registers (up to 1024
+ * threads), lean = 0 the one for 128 (up to 512).  YMFLOW_ERR_ARG otherwise.  YMFLOW_OPT_TIMED_REUNIT: the FP64
  * reunitarisation of the mixed forms after every n-th step of
  * ymflow_time_steps / ymflow_time_kernels (0 = none, the default), so timed
  * steps can carry it as ymflow_flow's reunit_every does.

@@ -9,7 +9,8 @@
 // and finishes the tile's links from there.
 //
 // Tiling.  A tile is Lx x Ty x Tz sites of one time slice (whole x lines, a
-// Ty x Tz patch of (y, z)), one thread per site.  A work unit is one tile
+// Ty x Tz patch of (y, z)); a thread advances 1, 2 or 4 of a site's links
+// (lpt), so a block has 4 ns / lpt threads.  A work unit is one tile
 // column (yb, zb) at one time t; a block owns a run of consecutive units, t
 // fastest, and streams through them along t:
 //   * the generators of the three planes (a, t) of slice t stay in shared
@@ -21,8 +22,8 @@
 //   * x - x is always inside (whole lines, periodic).
 // A unit's work: the plane generators of the tile (and faces, and the
 // previous slice's time planes where needed) into shared memory, a barrier,
-// then each thread advances its site's four links (rk_finish, shared with the
-// other stage kernels), a barrier.  Links go from `in` to `out` (ping-pong), so
+// then each thread advances its links (rk_finish, shared with the other stage
+// kernels), a barrier.  Links go from `in` to `out` (ping-pong), so
 // blocks never wait on one another.
 //
 // Against the two-kernel stage this removes the plaquette field's HBM round
@@ -93,10 +94,12 @@ __device__ __forceinline__ int yface_slot(int p) { return p == 0 ? 0 : p - 2; } 
 __device__ __forceinline__ int zface_slot(int p) { return p == 1 ? 0 : (p == 3 ? 1 : 2); }  // p in {1, 3, 5}
 
 // One work unit: tile column `col` of g at time t.  Every thread of the block
-// (nthreads >= tp.ns) takes part in the plane work and the barriers; threads
-// tid < tp.ns then own one site's four links.  `prologue`: the time planes of
-// slice t - 1 are not in shared memory yet (first unit of a run or of a
-// column).  `cur` selects which T buffer is slice t's.
+// takes part in the plane work and the barriers; threads [0, ns 4 / lpt) then
+// advance lpt links each: thread i the links (i / ns) lpt ... + lpt - 1 of
+// tile site i % ns (warp-uniform directions when ns is a multiple of 32).
+// `prologue`: the time planes of slice t - 1 are not in shared memory yet
+// (first unit of a run or of a column).  `cur` selects which T buffer is slice
+// t's.
 template <class F, int STAGE>
 __device__ __forceinline__ void tile_unit(const F& in, const F& out, const ForceField<typename F::Real>& zf,
                                           const Geo& g, const TileShape& tp, typename F::Real eps,
@@ -167,15 +170,17 @@ __device__ __forceinline__ void tile_unit(const F& in, const F& out, const Force
     }
     __syncthreads();
 
-    // The four links of the thread's site, each from the tile's plane generators.
-    if (tid < ns) {
-        const int x = tid % Lx;
-        const int jyz = tid / Lx;
+    // The thread's links, each from the tile's plane generators.
+    if (tid < ns * (4 / tp.lpt)) {
+        const int grp = tid / ns;
+        const int st = tid - grp * ns;  // the site within the tile
+        const int x = st % Lx;
+        const int jyz = st / Lx;
         const int jy = jyz % tp.ty, jz = jyz / tp.ty;
         const int c[4] = {x, y0 + jy, z0 + jz, t};
         const int s = x + g.stride[1] * c[1] + g.stride[2] * c[2] + g.stride[3] * t;
 #pragma unroll 1
-        for (int mu = 0; mu < 4; mu++) {
+        for (int mu = grp * tp.lpt; mu < (grp + 1) * tp.lpt; mu++) {
             Herm8<R> d;
             d.d0 = d.d1 = R(0);
             d.z01 = d.z02 = d.z12 = cx(R(0), R(0));
@@ -185,15 +190,15 @@ __device__ __forceinline__ void tile_unit(const F& in, const F& out, const Force
                 const int p = mu < nu ? plane_index(mu, nu) : plane_index(nu, mu);
                 const R sg = mu < nu ? R(1) : R(-1);
                 V* const own = plane_b(p) == 3 ? Tc + time_slot(p) * KU * ns : S + spatial_slot(p) * KU * ns;
-                const Herm8<R> upper = HV::get(own + tid, ns);
+                const Herm8<R> upper = HV::get(own + st, ns);
                 // H_p(x - nu): inside the tile, on a recomputed face, or slice t - 1
                 const V* lb = own;
                 int ln = ns, li;
                 if (nu == 0) {
-                    li = x == 0 ? tid + Lx - 1 : tid - 1;
+                    li = x == 0 ? st + Lx - 1 : st - 1;
                 } else if (nu == 1) {
                     if (jy > 0 || tp.nfy == 0) {
-                        li = jy > 0 ? tid - Lx : tid + Lx * (tp.ty - 1);
+                        li = jy > 0 ? st - Lx : st + Lx * (tp.ty - 1);
                     } else {
                         lb = FY + yface_slot(p) * KU * tp.nfy;
                         ln = tp.nfy;
@@ -201,7 +206,7 @@ __device__ __forceinline__ void tile_unit(const F& in, const F& out, const Force
                     }
                 } else if (nu == 2) {
                     if (jz > 0 || tp.nfz == 0) {
-                        li = jz > 0 ? tid - Lx * tp.ty : tid + Lx * tp.ty * (tp.tz - 1);
+                        li = jz > 0 ? st - Lx * tp.ty : st + Lx * tp.ty * (tp.tz - 1);
                     } else {
                         lb = FZ + zface_slot(p) * KU * tp.nfz;
                         ln = tp.nfz;
@@ -209,7 +214,7 @@ __device__ __forceinline__ void tile_unit(const F& in, const F& out, const Force
                     }
                 } else {
                     lb = Tp + time_slot(p) * KU * ns;
-                    li = tid;
+                    li = st;
                 }
                 const int y = g.hop_rt(s, g.coord(c, nu), nu, -1);
                 const M3<R> v = in.load(nu, y);

@@ -45,7 +45,10 @@ cudaError_t launch_rk_split_stage_halo(int prec, int stage, const void* uin, voi
 // of (tile column, t) units.
 struct TileShape {
     int ty, tz;      // tile extent in y and z
-    int ns;          // sites per tile = threads per block (Lx ty tz)
+    int ns;          // sites per tile (Lx ty tz)
+    int lpt;         // links a thread advances: 1, 2 or 4
+    int threads;     // threads per block: ns 4 / lpt (at most 1024)
+    int lean;        // 1: the kernel compiled for 64 registers (1024 threads, or two 512-thread blocks per SM)
     int nyt, nzt;    // tiles along y and z
     int nfy, nfz;    // sites of the recomputed lower y / z faces (0: the tile spans the extent)
     int units;       // tile columns x time slices
@@ -55,7 +58,8 @@ struct TileShape {
 // 64..512 threads, shared memory within 227 KB); fills *out (grid left 0).
 // whole_warps = false drops the warp rule (x-y runs of any length, 32..512
 // threads): correct, with warps straddling rows (the ensemble's 12^4).
-bool make_tile_shape(int prec, const Geo& g, int ty, int tz, TileShape* out, bool whole_warps = true);
+bool make_tile_shape(int prec, const Geo& g, int ty, int tz, TileShape* out, bool whole_warps = true, int lpt = 4,
+                     int lean = 0);
 size_t tile_smem_bytes(int prec, const TileShape& tp);
 // Opt the tile kernels of a precision into their shared memory (per device).
 cudaError_t prepare_tile_kernels(int prec);

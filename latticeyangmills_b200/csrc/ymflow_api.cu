@@ -106,7 +106,8 @@ namespace {
 
 // The tiling of the shared-memory stage kernel used by default: among the
 // (ty, tz) that tile the lattice into at least one unit per SM, the one with
-// the least recomputed face work per site (ties: the smaller tile).  false if
+// the least recomputed face work per site (ties: the smaller tile), two links
+// per thread on the 64-register kernel.  false if
 // none qualifies (small lattices, x extents whose lines do not fill whole
 // warps, slabs).
 bool default_tile(const ymflow_ctx* c, TileShape* out) {
@@ -120,7 +121,7 @@ bool default_tile(const ymflow_ctx* c, TileShape* out) {
     for (int ty = 1; ty <= c->geo.n[1]; ty++) {
         for (int tz = 1; tz <= c->geo.n[2]; tz++) {
             TileShape tp;
-            if (!make_tile_shape(c->prec, c->geo, ty, tz, &tp) || tp.units < sms) continue;
+            if (!make_tile_shape(c->prec, c->geo, ty, tz, &tp, true, 2, 1) || tp.units < sms) continue;
             const double cost = double(tp.nfy + tp.nfz) / tp.ns + 1e-6 * tp.ns;
             if (!found || cost < best) {
                 if (tile_grid(c->prec, c->device, &tp) != cudaSuccess) {
@@ -134,6 +135,11 @@ bool default_tile(const ymflow_ctx* c, TileShape* out) {
         }
     }
     return found;
+}
+
+// YMFLOW_OPT_TILE's value of a tiling
+int64_t tile_option(const TileShape& tp) {
+    return (int64_t(tp.lean) << 36) | (int64_t(tp.lpt) << 32) | (int64_t(tp.ty) << 16) | int64_t(tp.tz);
 }
 
 void drop_graphs(ymflow_ctx* c) {
@@ -346,23 +352,19 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     if (r == YMFLOW_OK) r = dev_alloc(c, &c->z, zb, "force buffer");
     if (r == YMFLOW_OK) r = dev_alloc(c, (void**)&c->deviation, sizeof(unsigned long long), "drift flag");
     // FP32 forms flow with the plaquette-field form of the force (fewer
-    // multiply-adds per link than the staple form): in one kernel with a
-    // tile's plane generators in shared memory where the lattice tiles into
-    // enough blocks to fill the GPU, else as two kernels through a stored
-    // plaquette field.  FP64 keeps the fused staple kernel, the faster form at
-    // its two-row staple products.  ymflow_autotune times every form.
+    // multiply-adds per link than the staple form) as two kernels through a
+    // stored plaquette field; FP64 keeps the fused staple kernel, the faster
+    // form at its two-row staple products.  The one-kernel form with a tile's
+    // plane generators in shared memory is prepared (its default tiling) for
+    // YMFLOW_OPT_STAGE_FORM 2 and the autotuner, which times every form.
     if (r == YMFLOW_OK && prepare_tile_kernels(c->prec) != cudaSuccess) {
         const cudaError_t e = cudaGetLastError();
         r = cuda_fail(c, e == cudaSuccess ? cudaErrorInvalidValue : e, "tile kernel set-up");
     }
     if (r == YMFLOW_OK) c->tile_ok = default_tile(c, &c->tile);
     if (r == YMFLOW_OK && c->prec != YMFLOW_FP64) {
-        if (c->tile_ok) {
-            c->stage_form = 2;
-        } else {
-            r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, V), "plaquette field");
-            c->stage_form = 1;
-        }
+        r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, V), "plaquette field");
+        c->stage_form = 1;
     }
     if (r == YMFLOW_OK) r = ensure_partials(c);
     if (r == YMFLOW_OK) r = ensure_meas(c, 16);
@@ -855,7 +857,8 @@ int time_stage0(ymflow_ctx* c, double eps, int reps, float* ms) {
 }
 
 struct TuneChoice {
-    int form, ty, tz;
+    int form;
+    int64_t tile;  // YMFLOW_OPT_TILE value (form 2)
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 6>, TuneChoice> g_tune_cache;  // (dims, precision, device) -> choice
@@ -874,7 +877,7 @@ int ymflow_autotune(ymflow_ctx* c, double eps, int* stage_form, int* tile_y, int
     const std::array<int, 6> key = {c->dims[0], c->dims[1], c->dims[2], c->dims[3], c->prec, c->device};
     auto apply = [&](const TuneChoice& ch) -> int {
         if (ch.form == 2) {
-            const int r = ymflow_set_option(c, YMFLOW_OPT_TILE, (int64_t(ch.ty) << 16) | ch.tz);
+            const int r = ymflow_set_option(c, YMFLOW_OPT_TILE, ch.tile);
             if (r != YMFLOW_OK) return r;
         }
         return ymflow_set_option(c, YMFLOW_OPT_STAGE_FORM, ch.form);
@@ -894,13 +897,16 @@ int ymflow_autotune(ymflow_ctx* c, double eps, int* stage_form, int* tile_y, int
         }
     }
     const bool had_hfield = c->hfield != nullptr;
-    std::vector<TuneChoice> cands = {{0, 0, 0}, {1, 0, 0}};
+    std::vector<TuneChoice> cands = {{0, 0}, {1, 0}};
     for (int ty = 1; ty <= c->geo.n[1]; ty++)
-        for (int tz = 1; tz <= c->geo.n[2]; tz++) {
-            TileShape tp;
-            if (make_tile_shape(c->prec, c->geo, ty, tz, &tp)) cands.push_back({2, ty, tz});
-        }
-    TuneChoice best = {c->stage_form, c->tile.ty, c->tile.tz};
+        for (int tz = 1; tz <= c->geo.n[2]; tz++)
+            for (int lpt : {1, 2, 4})
+                for (int lean : {0, 1}) {
+                    TileShape tp;
+                    if (make_tile_shape(c->prec, c->geo, ty, tz, &tp, true, lpt, lean))
+                        cands.push_back({2, tile_option(tp)});
+                }
+    TuneChoice best = {c->stage_form, c->tile_ok ? tile_option(c->tile) : 0};
     float best_ms = 0.f;
     bool any = false;
     for (const TuneChoice& ch : cands) {
@@ -963,9 +969,11 @@ int ymflow_set_option(ymflow_ctx* c, int key, int64_t value) {
             return YMFLOW_OK;
         }
         case YMFLOW_OPT_TILE: {
-            const int ty = int(value >> 16), tz = int(value & 0xffff);
+            const int ty = int((value >> 16) & 0xffff), tz = int(value & 0xffff);
+            const int lpt = int((value >> 32) & 0xf) ? int((value >> 32) & 0xf) : 4;
+            const int lean = int((value >> 36) & 1);
             TileShape tp;
-            if (value < 0 || value > 0x7fffffff || !make_tile_shape(c->prec, c->geo, ty, tz, &tp))
+            if (value < 0 || (value >> 37) != 0 || !make_tile_shape(c->prec, c->geo, ty, tz, &tp, true, lpt, lean))
                 return fail(c, YMFLOW_ERR_ARG, "tile (" + std::to_string(ty) + ", " + std::to_string(tz) +
                                                    ") does not tile this lattice's (y, z) in whole warps of x lines "
                                                    "within 64..512 threads and 227 KB of shared memory");
@@ -992,7 +1000,7 @@ int ymflow_get_option(const ymflow_ctx* c, int key, int64_t* value) {
         case YMFLOW_OPT_OBS_BLOCK: *value = 192; return YMFLOW_OK;
         case YMFLOW_OPT_GRAPH: *value = c->use_graph ? 1 : 0; return YMFLOW_OK;
         case YMFLOW_OPT_STAGE_FORM: *value = c->stage_form; return YMFLOW_OK;
-        case YMFLOW_OPT_TILE: *value = c->tile_ok ? (int64_t(c->tile.ty) << 16) | c->tile.tz : 0; return YMFLOW_OK;
+        case YMFLOW_OPT_TILE: *value = c->tile_ok ? tile_option(c->tile) : 0; return YMFLOW_OK;
         case YMFLOW_OPT_TIMED_REUNIT: *value = c->timed_reunit; return YMFLOW_OK;
         default: return YMFLOW_ERR_ARG;
     }

@@ -255,9 +255,11 @@ class GluonField:
                                              ctypes.byref(tz)))
         return f.value, ty.value, tz.value
 
-    def set_tile(self, ty: int, tz: int) -> None:
-        """The shared-memory stage kernel's tile (form 2), and that form."""
-        self.set_option(N.OPT_TILE, (int(ty) << 16) | int(tz))
+    def set_tile(self, ty: int, tz: int, lpt: int = 4, lean: int = 0) -> None:
+        """The shared-memory stage kernel's tile (form 2), and that form:
+        ty x tz x-lines per tile, lpt links per thread, lean = the 64-register
+        kernel."""
+        self.set_option(N.OPT_TILE, tile_option(ty, tz, lpt, lean))
         self.set_option(N.OPT_STAGE_FORM, N.STAGE_TILE)
 
     def device_bytes(self) -> int:
@@ -355,6 +357,11 @@ class Ensemble:
 
     def reset_time(self) -> None:
         self._check(N.load().ymflow_ensemble_reset_time(self._ens))
+
+
+def tile_option(ty: int, tz: int, lpt: int = 4, lean: int = 0) -> int:
+    """YMFLOW_OPT_TILE's value of a tiling."""
+    return (int(lean) << 36) | (int(lpt) << 32) | (int(ty) << 16) | int(tz)
 
 
 def _prefer_framework_nccl() -> None:

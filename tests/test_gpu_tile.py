@@ -2,8 +2,8 @@
 (YMFLOW_OPT_STAGE_FORM 2, csrc/flow_tile.cu).  In FP64 it is the reference's
 flow to 1e-12 against the golden tables; at every tiling (faces recomputed or
 wrapped inside the tile, runs of units streaming along t across columns) it
-equals the other forms to rounding; in FP32 (the default where a lattice
-tiles) it meets the accuracy target against the FP64 flow."""
+equals the other forms to rounding; in FP32 it meets the accuracy target
+against the FP64 flow."""
 import numpy as np
 import pytest
 
@@ -50,6 +50,9 @@ SHAPES = [
     ((32, 4, 6, 5), (2, 3)), ((32, 4, 6, 5), (4, 1)), ((32, 4, 6, 5), (1, 6)), ((32, 4, 6, 5), (4, 2)),
     ((32, 1, 3, 4), (1, 3)), ((32, 2, 2, 1), (2, 2)), ((16, 4, 4, 6), (2, 4)), ((8, 8, 4, 3), (4, 2)),
     ((64, 4, 4, 3), (2, 2)), ((32, 16, 16, 12), (2, 4)), ((32, 16, 16, 12), (2, 2)),
+    # one or two links per thread, the 64-register kernel
+    ((32, 4, 6, 5), (2, 3, 1, 1)), ((32, 4, 6, 5), (2, 3, 2, 1)), ((32, 16, 16, 12), (4, 4, 2, 1)),
+    ((32, 16, 16, 12), (4, 2, 2, 0)), ((16, 4, 4, 6), (2, 4, 1, 1)), ((32, 16, 16, 12), (2, 2, 4, 1)),
 ]
 
 
@@ -64,7 +67,8 @@ def test_fp64_tile_equals_fused_link_by_link(n, tile):
 
 
 @pytest.mark.parametrize("precision", ["fp32_18", "fp32_12"])
-@pytest.mark.parametrize("n,tile", [((32, 4, 6, 5), (2, 3)), ((32, 16, 16, 12), (4, 4)), ((16, 4, 4, 6), (2, 4))])
+@pytest.mark.parametrize("n,tile", [((32, 4, 6, 5), (2, 3)), ((32, 16, 16, 12), (4, 4)), ((16, 4, 4, 6), (2, 4)),
+                                    ((32, 16, 16, 12), (4, 4, 2, 1)), ((32, 16, 16, 12), (4, 2, 1, 1))])
 def test_fp32_tile_equals_two_kernel_form(precision, n, tile):
     """Same plaquette generators, same conjugations, same accumulation order as
     the two-kernel form: equal to FP32 rounding."""
@@ -77,15 +81,14 @@ def test_fp32_tile_equals_two_kernel_form(precision, n, tile):
 @pytest.mark.parametrize("precision", ["fp32_18", "fp32_12"])
 def test_fp32_tile_meets_the_accuracy_target_at_t4(precision):
     """32^4, U = e^{iaH} (a = 0.35), eps 0.01 to t = 4, reunitarisation every 10
-    steps, in the default form (the tile kernel): |d(t^2 E)| / t^2 E < 1e-6 and
+    steps, with the tile kernel: |d(t^2 E)| / t^2 E < 1e-6 and
     |dQ| < 1e-4 against the FP64 flow at t = 4; earlier rows within 1e-5."""
     from latticeyangmills_b200 import GluonField, _native as N
 
     n = (32, 32, 32, 32)
-    with GluonField(n, precision) as f:
-        assert f.get_option(N.OPT_STAGE_FORM) == 2
     r64, _ = flow_with(n, "fp64", steps=400, every=100, eps=0.01, seed=1, a=0.35)
-    r32, _ = flow_with(n, precision, steps=400, every=100, eps=0.01, seed=1, a=0.35, reunit=10)
+    r32, _ = flow_with(n, precision, tile=(4, 4, 2, 1), steps=400, every=100, eps=0.01, seed=1, a=0.35,
+                       reunit=10)
     rel = np.abs(r32[1:, 5] - r64[1:, 5]) / np.abs(r64[1:, 5])
     dq = np.abs(r32[:, 3] - r64[:, 3]).max()
     print(precision, "t", r32[1:, 1], "rel err t2E", rel, "|dQ|", dq)
@@ -96,20 +99,22 @@ def test_fp32_tile_meets_the_accuracy_target_at_t4(precision):
 
 
 def test_tile_defaults_and_refusals():
-    from latticeyangmills_b200 import GluonField, YmflowError, _native as N
+    from latticeyangmills_b200 import GluonField, YmflowError, _native as N, tile_option
 
     with GluonField((32, 32, 32, 32), "fp32_12") as f:
-        assert f.get_option(N.OPT_STAGE_FORM) == 2
-        assert f.get_option(N.OPT_TILE) == (4 << 16) | 4
+        assert f.get_option(N.OPT_STAGE_FORM) == 1
+        assert f.get_option(N.OPT_TILE) == tile_option(4, 4, 2, 1)  # the prepared default tiling
+        f.set_option(N.OPT_STAGE_FORM, 2)
     with GluonField((32, 32, 32, 32), "fp64") as f:
         assert f.get_option(N.OPT_STAGE_FORM) == 0
         f.set_tile(2, 2)
         assert f.get_option(N.OPT_STAGE_FORM) == 2
+        assert f.get_option(N.OPT_TILE) == tile_option(2, 2)
     with GluonField((16, 16, 16, 32), "fp32_18") as f:
-        assert f.get_option(N.OPT_STAGE_FORM) == 2
-        for bad in ((3, 2), (1, 4), (0, 1), (16, 16)):  # 3 does not divide 16; Lx ty < 32; zero; 4096 threads
+        # 3 does not divide 16; Lx ty < 32; zero; 4096 sites; 3 links a thread; 1024 threads on the 128-register kernel
+        for bad in ((3, 2), (1, 4), (0, 1), (16, 16), (4, 4, 3, 0), (8, 4, 1, 0)):
             with pytest.raises(YmflowError):
-                f.set_option(N.OPT_TILE, (bad[0] << 16) | bad[1])
+                f.set_option(N.OPT_TILE, tile_option(*bad))
     with GluonField((12, 12, 12, 12), "fp32_12") as f:  # 12-site x lines fill no whole warp
         assert f.get_option(N.OPT_STAGE_FORM) == 1
         with pytest.raises(YmflowError):
@@ -131,7 +136,7 @@ def test_autotune_picks_a_form_and_keeps_the_field():
         assert form in (0, 1, 2)
         assert f.get_option(N.OPT_STAGE_FORM) == form
         if form == 2:
-            assert f.get_option(N.OPT_TILE) == (ty << 16) | tz
+            assert (f.get_option(N.OPT_TILE) & 0xFFFFFFFF) == (ty << 16) | tz
         np.testing.assert_array_equal(f.download(), before)
         rows = f.flow(0.01, 4, 2, reunit_every=2)
     want, _ = flow_with(n, "fp32_12", form=1, steps=4, every=2, eps=0.01, seed=4, a=0.35, reunit=2)
@@ -152,4 +157,5 @@ def test_timed_steps_carry_the_reunitarisation():
         assert f.get_option(N.OPT_TIMED_REUNIT) == 10
         with_reunit, _ = f.time_steps(0.01, 20)
         el, field, stage = f.time_kernels(0.01, 20)
-    assert with_reunit > 0 and plain > 0 and el > 0 and stage > 0 and field < 0.01 * el
+    assert with_reunit > 0 and plain > 0 and el > 0 and stage > 0
+    assert field / (3 * 20) < 0.01  # back-to-back events around no kernel: microseconds per stage
