@@ -31,9 +31,15 @@
 
 namespace ym {
 
+// e^{iQ} = (1 + f0m1) + f1 Q + f2 Q^2.  The constant coefficient is kept as
+// f0 - 1, so that e^{iQ} - 1 (small for small Q) is formed without rounding a
+// 1 into it: an FP32 link update U + (e^{iQ} - 1) U then carries only the
+// rounding of the stored link, not that of e^{iQ}'s entries near 1, which
+// otherwise drifts the FP32 flow systematically (t^2 E about 1e-6 off at t = 2
+// with reunitarisation every 10 steps).
 template <class S>
 struct ChCoef {
-    Cx<S> f0, f1, f2;
+    Cx<S> f0m1, f1, f2;
 };
 
 template <class S>
@@ -51,11 +57,11 @@ __device__ __forceinline__ float ch_small_c1<float>() { return 1e-20f; }
 // the series of e^{iQ} itself: the error is below rho^{N+1}/(N+1)! e^rho with
 // rho the largest |eigenvalue| of Q, rho^2 <= 4 c1 / 3.  No transcendental
 // function, no division and no cancellation: every term is a small correction
-// to (1, i, -1/2).
+// to (1, i, -1/2), and f0 - 1 is the sum of the terms alone.
 template <class S, int N>
 __device__ __forceinline__ ChCoef<S> ch_series(S c0, S c1) {
     ChCoef<S> f;
-    f.f0 = cx(S(1), S(0));
+    f.f0m1 = cx(S(0), S(0));
     f.f1 = cx(S(0), S(1));
     f.f2 = cx(S(-0.5), S(0));
     S a = S(0), b = S(0), c = S(0.5);  // A_2/2!, B_2/2!, C_2/2!
@@ -69,10 +75,10 @@ __device__ __forceinline__ ChCoef<S> ch_series(S c0, S c1) {
         b = nb;
         c = nc;
         switch (n & 3) {  // i^n
-            case 0: f.f0.re += a; f.f1.re += b; f.f2.re += c; break;
-            case 1: f.f0.im += a; f.f1.im += b; f.f2.im += c; break;
-            case 2: f.f0.re -= a; f.f1.re -= b; f.f2.re -= c; break;
-            default: f.f0.im -= a; f.f1.im -= b; f.f2.im -= c; break;
+            case 0: f.f0m1.re += a; f.f1.re += b; f.f2.re += c; break;
+            case 1: f.f0m1.im += a; f.f1.im += b; f.f2.im += c; break;
+            case 2: f.f0m1.re -= a; f.f1.re -= b; f.f2.re -= c; break;
+            default: f.f0m1.im -= a; f.f1.im -= b; f.f2.im -= c; break;
         }
     }
     return f;
@@ -100,7 +106,7 @@ template <class S>
 __device__ __forceinline__ ChCoef<S> ch_coefficients(S c0, S c1) {
     ChCoef<S> f;
     if (!(c1 > ch_small_c1<S>())) {  // also catches NaN c1: falls to the series
-        f.f0 = cx(S(1), S(0));
+        f.f0m1 = cx(S(0), S(0));
         f.f1 = cx(S(0), S(1));
         f.f2 = cx(S(-0.5), S(0));
         return f;
@@ -138,7 +144,7 @@ __device__ __forceinline__ ChCoef<S> ch_coefficients(S c0, S c1) {
         h2i = -h2i;
     }
     const S norm = S(1) / (S(9) * u2 - w2);
-    f.f0 = cx(h0r * norm, h0i * norm);
+    f.f0m1 = cx(h0r * norm - S(1), h0i * norm);
     f.f1 = cx(h1r * norm, h1i * norm);
     f.f2 = cx(h2r * norm, h2i * norm);
     return f;
@@ -218,7 +224,7 @@ __device__ __forceinline__ ChCoef<float> exp_coefficients<float>(const Herm8<flo
     if (x < float(YM_DEGENERATE_X) && c1 > 1e-12f) return ch_coefficients<float>(c0, c1);
     ChCoef<double> d = ch_coefficients<double>(herm_det<double>(q, q22), herm_c1<double>(q, q22));
     ChCoef<float> f;
-    f.f0 = cx(float(d.f0.re), float(d.f0.im));
+    f.f0m1 = cx(float(d.f0m1.re), float(d.f0m1.im));
     f.f1 = cx(float(d.f1.re), float(d.f1.im));
     f.f2 = cx(float(d.f2.re), float(d.f2.im));
     return f;
@@ -230,10 +236,10 @@ __device__ __forceinline__ void exp_iq(const Herm8<R>& q, M3<R>& e) {
     const R q22 = -(q.d0 + q.d1);
     const ChCoef<R> f = exp_coefficients<R>(q, q22);
     const QSquared<R> s = q_squared(q, q22);
-    // diagonal: f0 + f1 q_ii + f2 (Q^2)_ii  (q_ii and (Q^2)_ii real)
-    e.e[0][0] = cx(f.f0.re + f.f1.re * q.d0 + f.f2.re * s.a00, f.f0.im + f.f1.im * q.d0 + f.f2.im * s.a00);
-    e.e[1][1] = cx(f.f0.re + f.f1.re * q.d1 + f.f2.re * s.a11, f.f0.im + f.f1.im * q.d1 + f.f2.im * s.a11);
-    e.e[2][2] = cx(f.f0.re + f.f1.re * q22 + f.f2.re * s.a22, f.f0.im + f.f1.im * q22 + f.f2.im * s.a22);
+    // diagonal: 1 + f0m1 + f1 q_ii + f2 (Q^2)_ii  (q_ii and (Q^2)_ii real)
+    e.e[0][0] = cx(R(1) + (f.f0m1.re + f.f1.re * q.d0 + f.f2.re * s.a00), f.f0m1.im + f.f1.im * q.d0 + f.f2.im * s.a00);
+    e.e[1][1] = cx(R(1) + (f.f0m1.re + f.f1.re * q.d1 + f.f2.re * s.a11), f.f0m1.im + f.f1.im * q.d1 + f.f2.im * s.a11);
+    e.e[2][2] = cx(R(1) + (f.f0m1.re + f.f1.re * q22 + f.f2.re * s.a22), f.f0m1.im + f.f1.im * q22 + f.f2.im * s.a22);
     // off-diagonal: f1 q_ij + f2 (Q^2)_ij; lower entries use the conjugates of q and Q^2
 #define YM_OFFD(I, J, QV, SV)                                                                     \
     e.e[I][J] = cx(f.f1.re * QV.re - f.f1.im * QV.im + f.f2.re * SV.re - f.f2.im * SV.im,         \
@@ -246,14 +252,15 @@ __device__ __forceinline__ void exp_iq(const Herm8<R>& q, M3<R>& e) {
 #undef YM_OFFD
 }
 
-// Rows 0 and 1 of e^{iQ} (enough to update an SU(3) link through its first two rows).
+// Rows 0 and 1 of e^{iQ} - 1 (enough to update an SU(3) link through its
+// first two rows as U + (e^{iQ} - 1) U).
 template <class R>
-__device__ __forceinline__ void exp_iq_rows2(const Herm8<R>& q, Rows2<R>& e) {
+__device__ __forceinline__ void expm1_iq_rows2(const Herm8<R>& q, Rows2<R>& e) {
     const R q22 = -(q.d0 + q.d1);
     const ChCoef<R> f = exp_coefficients<R>(q, q22);
     const QSquared<R> s = q_squared(q, q22);
-    e.e[0][0] = cx(f.f0.re + f.f1.re * q.d0 + f.f2.re * s.a00, f.f0.im + f.f1.im * q.d0 + f.f2.im * s.a00);
-    e.e[1][1] = cx(f.f0.re + f.f1.re * q.d1 + f.f2.re * s.a11, f.f0.im + f.f1.im * q.d1 + f.f2.im * s.a11);
+    e.e[0][0] = cx(f.f0m1.re + f.f1.re * q.d0 + f.f2.re * s.a00, f.f0m1.im + f.f1.im * q.d0 + f.f2.im * s.a00);
+    e.e[1][1] = cx(f.f0m1.re + f.f1.re * q.d1 + f.f2.re * s.a11, f.f0m1.im + f.f1.im * q.d1 + f.f2.im * s.a11);
     // upper entries f1 q_ij + f2 (Q^2)_ij; e10 from the conjugates of q01 and (Q^2)_01
     e.e[0][1] = cx(f.f1.re * q.z01.re - f.f1.im * q.z01.im + f.f2.re * s.a01.re - f.f2.im * s.a01.im,
                    f.f1.re * q.z01.im + f.f1.im * q.z01.re + f.f2.re * s.a01.im + f.f2.im * s.a01.re);

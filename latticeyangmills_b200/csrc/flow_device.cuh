@@ -136,9 +136,16 @@ __device__ __forceinline__ Rows2<typename F::Real> rk_finish(const F& out, const
         z = h8_axpby(R(3.0 / 4.0), dz, R(1.0), zf.load(mu, s));
     }
     const Herm8<R> q = h8_scale(eps, z);
-    Rows2<R> e, un;
-    exp_iq_rows2(q, e);
-    mmul_rows2<false, false>(e, u, un);  // e^{iQ} U is in SU(3): two rows suffice
+    Rows2<R> d, un;
+    expm1_iq_rows2(q, d);
+    mmul_rows2<false, false>(d, u, un);  // e^{iQ} U = U + (e^{iQ} - 1) U is in SU(3): two rows suffice
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            un.e[i][j].re += u.e[i][j].re;
+            un.e[i][j].im += u.e[i][j].im;
+        }
     out.store_rows2(mu, s, un);
     return un;
 }

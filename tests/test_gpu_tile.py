@@ -51,7 +51,7 @@ SHAPES = [
     ((32, 1, 3, 4), (1, 3)), ((32, 2, 2, 1), (2, 2)), ((16, 4, 4, 6), (2, 4)), ((8, 8, 4, 3), (4, 2)),
     ((64, 4, 4, 3), (2, 2)), ((32, 16, 16, 12), (2, 4)), ((32, 16, 16, 12), (2, 2)),
     # one or two links per thread, the 64-register kernel
-    ((32, 4, 6, 5), (2, 3, 1, 1)), ((32, 4, 6, 5), (2, 3, 2, 1)), ((32, 16, 16, 12), (4, 4, 2, 1)),
+    ((32, 4, 6, 5), (2, 3, 1, 1)), ((32, 4, 6, 5), (2, 3, 2, 1)), ((32, 16, 16, 12), (2, 2, 2, 1)),
     ((32, 16, 16, 12), (4, 2, 2, 0)), ((16, 4, 4, 6), (2, 4, 1, 1)), ((32, 16, 16, 12), (2, 2, 4, 1)),
 ]
 
