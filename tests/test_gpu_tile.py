@@ -158,4 +158,5 @@ def test_timed_steps_carry_the_reunitarisation():
         with_reunit, _ = f.time_steps(0.01, 20)
         el, field, stage = f.time_kernels(0.01, 20)
     assert with_reunit > 0 and plain > 0 and el > 0 and stage > 0
-    assert field / (3 * 20) < 0.01  # back-to-back events around no kernel: microseconds per stage
+    # the instrumented pass: the stage kernels inside the step time, which also holds two reunitarisations
+    assert field + stage < el
