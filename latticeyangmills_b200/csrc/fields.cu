@@ -288,10 +288,21 @@ __global__ void reunit_kernel(F u, int V, unsigned long long* deviation) {
             for (int j = 0; j < 3; j++) r.e[i][j] = cx(R(m.e[i][j].re), R(m.e[i][j].im));
         u.store(mu, s, r);
     }
-    // warp max, then one atomic per warp (non-negative doubles order like their bit patterns)
+    // Warp max, then block max, then one atomic per block, and only where the
+    // block's max exceeds the value already recorded: a few hundred atomics on
+    // one address per launch instead of one per warp (131,072 at 32^4), which
+    // serialised in L2 and made the launch several times its memory time.
+    // Non-negative doubles order like their bit patterns.
+    __shared__ double warp_max[32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dev = fmax(dev, __shfl_down_sync(0xffffffffu, dev, o));
-    if ((threadIdx.x & 31) == 0 && deviation) atomicMax(deviation, (unsigned long long)__double_as_longlong(dev));
+    if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x >> 5] = dev;
+    __syncthreads();
+    if (threadIdx.x == 0 && deviation) {
+        for (int w = 1; w < int(blockDim.x >> 5); w++) dev = fmax(dev, warp_max[w]);
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(dev);
+        if (bits > *reinterpret_cast<volatile unsigned long long*>(deviation)) atomicMax(deviation, bits);
+    }
 }
 
 cudaError_t launch_reunitarize(int prec, void* u, const Geo& g, unsigned long long* deviation, cudaStream_t st) {
