@@ -2,15 +2,19 @@
 vs FP64, on B200.
 
 One "step" is one Luscher RK3 flow step over a whole 32^4 configuration:
-4 * 32^4 = 4,194,304 link-updates.  Per stage the mixed forms run two kernels
-(the plaquette field, then the stage built on it); FP64 runs one fused kernel.
-The default precision is the 12-real FP32 form, the fastest that holds the
-1e-6 accuracy target.  Inputs are seeded
+4 * 32^4 = 4,194,304 link-updates; the mixed forms reunitarise in FP64 after
+every 10th step inside the timed region (the 32^4 configuration's schedule).
+The stage form (fused kernel, two kernels through a stored plaquette field,
+or one kernel with a tile's plaquette field in shared memory) is the
+project's autotuner's choice for the lattice and precision; on B200 it picks
+the two-kernel stage for FP32 and the fused kernel for FP64.  The default
+precision is the 12-real FP32 form.  Inputs are seeded
 synthetic fields U = e^{i a H} (a = 0.35, H Gaussian traceless Hermitian per
 link), generated on the device; 32^4 links plus the generator field are larger
 than the 126 MB L2 (no flush needed).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32_12|fp32_18|fp64]
+                  [--no-autotune | --stage-form 0|1|2 [--tile ty,tz,lpt,lean]]
   python bench.py --impl reference     # the reference's own CPU code on the host cores
 
 Multi-GPU (torchrun, one rank per GPU): every rank flows its own configuration
@@ -26,9 +30,12 @@ the single slab exchanges with itself, which prices the exchange on one GPU.
   python bench.py --workload 8 | 16x32 | 64   # the other configurations, every precision against FP64
   python bench.py --profile [--profile-kernel obs] --precision P   # only the timed kernels, for ncu
 
-The JSON line carries, besides the contract's keys: `roofline` (HBM, the
-stage kernel's algorithmic bytes over its event-timed launches; `field_kernel`
-the same for the plaquette-field kernel of the two-kernel stage),
+The JSON line carries, besides the contract's keys: `roofline` (HBM: the
+compulsory bytes of a stage, 6 s_U + 4 s_Z per link-update over three
+launches, over the stage kernel's time in the graph-replayed steps, `frac`;
+the whole step's fraction, `step_frac_8d`; the DRAM bytes the ncu captures in
+profiles/ count, over the compulsory ones; `field_kernel` the plaquette-field
+kernel of the two-kernel stage on its own bytes),
 `alu_roofline` (the reference algorithm's flops over the step's kernel time,
 against the measured FP32 or FP64 FMA peak),
 `accuracy_vs_fp64` (t^2 E and Q at t = 4), `ensemble` (64 configurations of
@@ -450,8 +457,13 @@ def our_arm(args, dist: Dist):
         if dist.rank == 0:
             print(json.dumps({"profile": True, "kernel": "observables", "precision": prec, "lattice": list(DIMS)}))
         return
-    # the stage form and tile: the project's autotuner (cached per lattice and precision)
-    tuned = None if args.no_autotune else f.autotune(EPS)
+    # the stage form and tile: the project's autotuner (cached per lattice and
+    # precision), or the one given on the command line
+    if args.stage_form is not None:
+        if args.stage_form == 2 and args.tile:
+            f.set_tile(*[int(v) for v in args.tile.split(",")])
+        f.set_option(N.OPT_STAGE_FORM, args.stage_form)
+    tuned = None if (args.no_autotune or args.stage_form is not None) else f.autotune(EPS)
     form = f.get_option(N.OPT_STAGE_FORM)
     tile = f.get_option(N.OPT_TILE)
     f.set_option(N.OPT_TIMED_REUNIT, reunit)  # the FP64 reunitarisation of the mixed forms, every 10 steps
@@ -712,7 +724,7 @@ def decomposed_run(args, dist: Dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32_12", choices=["fp64", "fp32_18", "fp32_12"])
@@ -729,6 +741,10 @@ def main():
                     help="one 32^4 configuration split along t over the ranks (NCCL halo exchange)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default stage form instead of the autotuner's choice")
+    ap.add_argument("--stage-form", type=int, choices=[0, 1, 2], default=None,
+                    help="run this stage form (0 fused, 1 two kernels, 2 shared-memory tile) instead of the "
+                         "autotuner's choice")
+    ap.add_argument("--tile", default=None, help="with --stage-form 2: ty,tz[,links per thread[,lean]]")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps of one precision (for ncu captures)")
     args = ap.parse_args()
