@@ -294,6 +294,32 @@ YMFLOW_API int ymflow_slab_connect(ymflow_ctx* ctx, const void* id, int rank, in
 YMFLOW_API int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nsteps, int measure_every,
                                       int reunit_every, ymflow_obs* out, int out_cap, int* n_out);
 
+/* --- One configuration split in any set of directions (blocks) ---------- */
+/* A block context holds the sites [origin, origin + extent) of a configuration
+ * of extents global_dims (extent = global in a direction the decomposition
+ * does not split) in a local lattice with one halo layer on each side of every
+ * split direction.  It replaces the reference's Cartesian domain decomposition
+ * in full (src/ParallelTools/parallel.cpp:57-100, SubLatticeSize in any
+ * direction, with the second-neighbour exchange of the clover, :117-140) for
+ * the blocks of one process on one or several GPUs.  ymflow_upload /
+ * ymflow_download / _sites address the block's own sites in lexicographic
+ * order over its extents (.bin layout); ymflow_init_links, ymflow_load_file,
+ * ymflow_flow and ymflow_observables of a single block return an error
+ * (flow and measure the group). */
+YMFLOW_API ymflow_ctx* ymflow_create_block(const int global_dims[4], const int origin[4], const int extent[4],
+                                           int precision, int device, int* status);
+
+/* ymflow_flow over the n = grid[0] grid[1] grid[2] grid[3] blocks of one
+ * configuration held in this process, ctxs[i] at grid coordinates
+ * (i % grid[0], i / grid[0] % grid[1], ...) with origins increasing along each
+ * direction; blocks on different GPUs must reach each other's memory.  After
+ * every stage each block pulls its halos from its neighbours, one split
+ * direction at a time, which also fills the edges the staples and the clover
+ * read.  Rows as ymflow_flow's, for the whole configuration. */
+YMFLOW_API int ymflow_block_group_flow(ymflow_ctx* const* ctxs, int n, const int grid[4], double eps, int nsteps,
+                                       int measure_every, int reunit_every, ymflow_obs* out, int out_cap,
+                                       int* n_out);
+
 /* Measured CUDA-core FMA throughput of `device` in TFLOP/s (2 flops per FMA):
  * FP64 FMAs for YMFLOW_FP64, FP32 FMAs otherwise.  A measurement utility with
  * no counterpart in the reference: the denominator of the stage kernels'

@@ -46,8 +46,10 @@ EXPORTS = (
     "ymflow_ensemble_flow", "ymflow_ensemble_reset_time", "ymflow_ensemble_time_steps",
     "ymflow_ensemble_autotune", "ymflow_ensemble_tuning", "ymflow_ensemble_set_tuning", "ymflow_observables_noalloc",
     "ymflow_create_slab", "ymflow_nccl_unique_id", "ymflow_slab_connect", "ymflow_slab_group_flow",
+    "ymflow_create_block", "ymflow_block_group_flow",
 )
-NON_INT = ("ymflow_version", "ymflow_create", "ymflow_create_slab", "ymflow_destroy", "ymflow_last_error",
+NON_INT = ("ymflow_version", "ymflow_create", "ymflow_create_slab", "ymflow_create_block", "ymflow_destroy",
+           "ymflow_last_error",
            "ymflow_ensemble_create",
            "ymflow_ensemble_destroy", "ymflow_ensemble_last_error")
 
@@ -147,6 +149,10 @@ def load():
     l.ymflow_slab_connect.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     l.ymflow_slab_group_flow.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(Obs), ctypes.c_int, IP]
+    l.ymflow_create_block.argtypes = [IP, IP, IP, ctypes.c_int, ctypes.c_int, IP]
+    l.ymflow_create_block.restype = vp
+    l.ymflow_block_group_flow.argtypes = [ctypes.POINTER(vp), ctypes.c_int, IP, ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(Obs), ctypes.c_int, IP]
     for name in EXPORTS:
         if name not in NON_INT:
             getattr(l, name).restype = ctypes.c_int

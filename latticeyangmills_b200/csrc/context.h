@@ -51,6 +51,12 @@ struct ymflow_ctx {
     bool slab = false;
     int t0 = 0, nt = 0;
     int gdims[4] = {0, 0, 0, 0};
+    // One block of a configuration decomposed in several directions
+    // (ymflow_create_block): its own sites [origin, origin + extent) of the
+    // configuration, held in a local lattice with one halo layer on each side
+    // in every direction the decomposition splits (geo.halo_mask).
+    bool is_block = false;
+    int borigin[4] = {0, 0, 0, 0};
     void* comm = nullptr;             // NCCL communicator (ymflow_slab_connect)
     int rank = 0, nranks = 0, lower = -1, upper = -1;
     int64_t bytes = 0;
@@ -60,6 +66,8 @@ struct ymflow_ctx {
 namespace ym {
 
 int fail(ymflow_ctx* c, int code, const std::string& msg);
+// The text ymflow_last_error(NULL) returns after a failed constructor.
+void set_create_error(const std::string& msg);
 int cuda_fail(ymflow_ctx* c, cudaError_t e, const char* what);
 
 #define YM_CK(ctx, call, what)                                      \
@@ -69,6 +77,9 @@ int cuda_fail(ymflow_ctx* c, cudaError_t e, const char* what);
     } while (0)
 
 int ensure_meas(ymflow_ctx* c, int rows);
+// One RK3 stage (0, 1, 2) of the context's stage form from link buffer `in`
+// into `out` over all of the context's sites.
+cudaError_t enqueue_stage(ymflow_ctx* c, int stage, const void* in, void* out, double eps);
 // Observables of the current field (the context's sites) into measurement row `row` on the device.
 int enqueue_measure(ymflow_ctx* c, int row);
 void fill_obs(const ymflow_ctx* c, const double* m, int64_t step, double t, ymflow_obs* o);

@@ -67,6 +67,34 @@ struct Geo {
     // link read as a time neighbour is read again a few hundred blocks later,
     // still in L2 (tile_groups divides slice_groups, the groups per time slice).
     int slice_groups, tile_groups;
+    // A block of a configuration decomposed in several directions
+    // (ymflow_create_block): bit d of halo_mask set where the local lattice
+    // carries one halo layer on each side in direction d; bext[] the block's
+    // own extents (the local extents less the halos).  0 / unused otherwise.
+    int halo_mask;
+    int bext[4];
+
+    // whether site coordinates c are the block's own (not a halo)
+    __device__ __forceinline__ bool interior(const int c[4]) const {
+        if (!halo_mask) return true;
+#pragma unroll
+        for (int d = 0; d < 4; d++)
+            if (((halo_mask >> d) & 1) && (c[d] == 0 || c[d] == n[d] - 1)) return false;
+        return true;
+    }
+    // local site of the block's k-th own site (own sites in lexicographic order, x fastest)
+    __device__ __forceinline__ int own_site(int k) const {
+        if (!halo_mask) return k;
+        int s = 0;
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const int q = k / bext[d];
+            const int cd = k - q * bext[d] + ((halo_mask >> d) & 1);
+            k = q;
+            s += cd * stride[d];
+        }
+        return s;
+    }
 
     __device__ __forceinline__ int block_group(int b) const {
         if (tile_groups == 0) return b;
@@ -130,6 +158,8 @@ inline Geo make_geo(const int dims[4]) {
     const int vs = dims[0] * dims[1] * dims[2];
     g.slice_groups = vs % 32 == 0 ? vs / 32 : 0;
     g.tile_groups = 0;
+    g.halo_mask = 0;
+    for (int i = 0; i < 4; i++) g.bext[i] = dims[i];
     return g;
 }
 

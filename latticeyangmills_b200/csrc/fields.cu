@@ -20,10 +20,10 @@ __device__ __forceinline__ double reverse_bytes(double x) {
 
 // Sites [first, first + n) of a .bin-layout block (aos points at site `first`).
 template <class F>
-__global__ void pack_kernel(const double* __restrict__ aos, F u, int first, int n, bool swap) {
+__global__ void pack_kernel(const double* __restrict__ aos, F u, Geo g, int first, int n, bool swap) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (l >= 4 * int64_t(n)) return;
-    const int s = first + int(l >> 2);
+    const int s = g.own_site(first + int(l >> 2));
     const int mu = int(l & 3);
     const double2* src = reinterpret_cast<const double2*>(aos + l * 18);
     M3<typename F::Real> a;
@@ -37,10 +37,10 @@ __global__ void pack_kernel(const double* __restrict__ aos, F u, int first, int 
 }
 
 template <class F>
-__global__ void unpack_kernel(F u, double* __restrict__ aos, int first, int n, bool swap) {
+__global__ void unpack_kernel(F u, Geo g, double* __restrict__ aos, int first, int n, bool swap) {
     const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (l >= 4 * int64_t(n)) return;
-    const int s = first + int(l >> 2);
+    const int s = g.own_site(first + int(l >> 2));
     const int mu = int(l & 3);
     const M3<typename F::Real> a = u.load(mu, s);
     double2* dst = reinterpret_cast<double2*>(aos + l * 18);
@@ -54,15 +54,15 @@ __global__ void unpack_kernel(F u, double* __restrict__ aos, int first, int n, b
 
 cudaError_t launch_pack_range(int prec, const double* aos, void* u, const Geo& g, int first, int n, bool swap,
                               cudaStream_t st) {
-    if (first < 0 || n < 0 || int64_t(first) + n > g.V) return cudaErrorInvalidValue;
+    if (first < 0 || n < 0 || int64_t(first) + n > g.V) return cudaErrorInvalidValue;  // (own sites <= V)
     if (n == 0) return cudaSuccess;
     const int b = 256;
     const unsigned nb = unsigned((4 * int64_t(n) + b - 1) / b);
     void* v = const_cast<void*>((const void*)u);
     switch (prec) {
-        case kFP64: pack_kernel<<<nb, b, 0, st>>>(aos, FieldD18{v, g.V}, first, n, swap); break;
-        case kFP32_18: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF18{v, g.V}, first, n, swap); break;
-        case kFP32_12: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF12{v, g.V}, first, n, swap); break;
+        case kFP64: pack_kernel<<<nb, b, 0, st>>>(aos, FieldD18{v, g.V}, g, first, n, swap); break;
+        case kFP32_18: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF18{v, g.V}, g, first, n, swap); break;
+        case kFP32_12: pack_kernel<<<nb, b, 0, st>>>(aos, FieldF12{v, g.V}, g, first, n, swap); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -70,15 +70,15 @@ cudaError_t launch_pack_range(int prec, const double* aos, void* u, const Geo& g
 
 cudaError_t launch_unpack_range(int prec, const void* u, double* aos, const Geo& g, int first, int n, bool swap,
                                 cudaStream_t st) {
-    if (first < 0 || n < 0 || int64_t(first) + n > g.V) return cudaErrorInvalidValue;
+    if (first < 0 || n < 0 || int64_t(first) + n > g.V) return cudaErrorInvalidValue;  // (own sites <= V)
     if (n == 0) return cudaSuccess;
     const int b = 256;
     const unsigned nb = unsigned((4 * int64_t(n) + b - 1) / b);
     void* v = const_cast<void*>(u);
     switch (prec) {
-        case kFP64: unpack_kernel<<<nb, b, 0, st>>>(FieldD18{v, g.V}, aos, first, n, swap); break;
-        case kFP32_18: unpack_kernel<<<nb, b, 0, st>>>(FieldF18{v, g.V}, aos, first, n, swap); break;
-        case kFP32_12: unpack_kernel<<<nb, b, 0, st>>>(FieldF12{v, g.V}, aos, first, n, swap); break;
+        case kFP64: unpack_kernel<<<nb, b, 0, st>>>(FieldD18{v, g.V}, g, aos, first, n, swap); break;
+        case kFP32_18: unpack_kernel<<<nb, b, 0, st>>>(FieldF18{v, g.V}, g, aos, first, n, swap); break;
+        case kFP32_12: unpack_kernel<<<nb, b, 0, st>>>(FieldF12{v, g.V}, g, aos, first, n, swap); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -208,10 +208,11 @@ __global__ void __launch_bounds__(kObsThreads, kObsMinBlocks)
     double plaq = 0.0, energy = 0.0, topc = 0.0;
     for (int grp = blockIdx.x; grp < groups; grp += gridDim.x) {  // block-uniform trip count
         int s = g.site0 + grp * kObsSites + lane;
-        const bool active = s < g.site1;
+        bool active = s < g.site1;
         if (!active) s = g.site0;  // computed but not counted: every thread reaches the barriers
         int c[4];
         g.coords(s, c);
+        active = active && g.interior(c);  // a block's halo sites are its neighbours'
         R pl;
         const AH<R> G = clover(u, g, s, c, MU, NU, pl);
         if (active) {

@@ -35,6 +35,7 @@ namespace {
 
 thread_local std::string g_create_error;
 
+
 int64_t link_count(const ymflow_ctx* c) { return 4 * c->geo.V; }
 
 int dev_alloc(ymflow_ctx* c, void** p, size_t bytes, const char* what) {
@@ -77,6 +78,10 @@ int ensure_partials(ymflow_ctx* c) {
 }
 
 }  // namespace
+
+namespace ym {
+void set_create_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace ym
 
 namespace ym {
 
@@ -241,6 +246,16 @@ int run_step(ymflow_ctx* c, double eps, cudaEvent_t* ev) {
 
 namespace ym {
 
+cudaError_t enqueue_stage(ymflow_ctx* c, int stage, const void* in, void* out, double eps) {
+    if (c->stage_form == 1) {
+        const cudaError_t e = launch_plaq_field(c->prec, in, c->hfield, c->geo, c->stream);
+        if (e != cudaSuccess) return e;
+        return launch_rk_split_stage(c->prec, stage, in, out, c->z, c->hfield, c->geo, eps, c->stream);
+    }
+    if (c->stage_form == 2) return launch_rk_tile_stage(c->prec, stage, in, out, c->z, c->geo, c->tile, eps, c->stream);
+    return launch_rk_stage(c->prec, stage, in, out, c->z, c->geo, eps, c->block, c->stream);
+}
+
 // Observables of the current field into meas row `row` (device).
 int enqueue_measure(ymflow_ctx* c, int row) {
     int r = ensure_partials(c);
@@ -267,6 +282,8 @@ void fill_obs(const ymflow_ctx* c, const double* m, int64_t step, double t, ymfl
 // A slab measures and flows only once connected; its halos are refreshed from
 // the neighbours first (the field may have been uploaded or initialised since).
 int slab_prepare(ymflow_ctx* c) {
+    if (c->is_block)
+        return fail(c, YMFLOW_ERR_STATE, "block context: flow and measure its group with ymflow_block_group_flow");
     if (!c->slab) return YMFLOW_OK;
     if (!c->comm)
         return fail(c, YMFLOW_ERR_STATE,
@@ -460,11 +477,17 @@ const char* ymflow_last_error(const ymflow_ctx* c) {
 
 int ymflow_upload(ymflow_ctx* c, const double* links) {
     if (!c || !links) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_upload");
+    if (c->is_block)
+        return ymflow_upload_sites(c, links, 0,
+                                   int64_t(c->geo.bext[0]) * c->geo.bext[1] * c->geo.bext[2] * c->geo.bext[3], 0);
     return ymflow_upload_sites(c, links, 0, int64_t(c->geo.site1 - c->geo.site0), 0);
 }
 
 int ymflow_download(ymflow_ctx* c, double* links) {
     if (!c || !links) return fail(c, YMFLOW_ERR_ARG, "null argument to ymflow_download");
+    if (c->is_block)
+        return ymflow_download_sites(c, links, 0,
+                                     int64_t(c->geo.bext[0]) * c->geo.bext[1] * c->geo.bext[2] * c->geo.bext[3], 0);
     return ymflow_download_sites(c, links, 0, int64_t(c->geo.site1 - c->geo.site0), 0);
 }
 
@@ -473,8 +496,10 @@ namespace {
 int check_site_range(ymflow_ctx* c, const void* p, int64_t first, int64_t n, int flags) {
     if (!c) return YMFLOW_ERR_ARG;
     if (!p && n > 0) return fail(c, YMFLOW_ERR_ARG, "null links pointer");
-    if (first < 0 || n < 0 || first + n > int64_t(c->geo.site1 - c->geo.site0))
-        return fail(c, YMFLOW_ERR_ARG, "site range outside the lattice (or the slab)");
+    const int64_t own = c->is_block ? int64_t(c->geo.bext[0]) * c->geo.bext[1] * c->geo.bext[2] * c->geo.bext[3]
+                                 : int64_t(c->geo.site1 - c->geo.site0);
+    if (first < 0 || n < 0 || first + n > own)
+        return fail(c, YMFLOW_ERR_ARG, "site range outside the lattice (or the slab / block)");
     if (flags & ~YMFLOW_IO_BIG_ENDIAN) return fail(c, YMFLOW_ERR_ARG, "unknown flags");
     return YMFLOW_OK;
 }
@@ -485,6 +510,8 @@ int ymflow_load_file(ymflow_ctx* c, const char* path, int flags, int64_t chunk_s
     NvtxRange range("ymflow_load_file");
     if (!c || !path) return YMFLOW_ERR_ARG;
     if (flags & ~YMFLOW_IO_BIG_ENDIAN) return fail(c, YMFLOW_ERR_ARG, "unknown flags");
+    if (c->is_block)
+        return fail(c, YMFLOW_ERR_STATE, "a block's sites are not one run of the file: upload them (ymflow_upload)");
     const int64_t n = c->geo.site1 - c->geo.site0;  // this context's sites
     const int64_t site_bytes = 4 * 18 * int64_t(sizeof(double));
     const int64_t chunk = std::min<int64_t>(chunk_sites > 0 ? chunk_sites : 65536, n);
@@ -590,6 +617,7 @@ int ymflow_init_links(ymflow_ctx* c, int kind, double a, uint64_t seed, uint32_t
     if (!c) return YMFLOW_ERR_ARG;
     if (kind != YMFLOW_FIELD_COLD && kind != YMFLOW_FIELD_EXPIAH) return fail(c, YMFLOW_ERR_ARG, "unknown field kind");
     if (!(haar_frac >= 0.0 && haar_frac <= 1.0)) return fail(c, YMFLOW_ERR_ARG, "haar_frac outside [0, 1]");
+    if (c->is_block) return fail(c, YMFLOW_ERR_STATE, "seeded fields fill whole lattices and slabs; upload a block's part");
     DeviceGuard guard(c->device);
     YM_CK(c, launch_init_links(c->prec, c->u[c->cur], c->geo, kind == YMFLOW_FIELD_COLD ? kCold : kExpIAH, a, seed,
                                config, c->stream),
@@ -607,7 +635,8 @@ int ymflow_generate_metropolis(ymflow_ctx* c, int start, double beta, double su3
                                uint64_t seed, double* acceptance) {
     NvtxRange range("ymflow_generate_metropolis");
     if (!c) return YMFLOW_ERR_ARG;
-    if (c->slab) return fail(c, YMFLOW_ERR_STATE, "generation runs on a whole-lattice context, not a slab");
+    if (c->slab || c->is_block)
+        return fail(c, YMFLOW_ERR_STATE, "generation runs on a whole-lattice context, not a slab or block");
     if (sweeps < 0 || hits < 1 || !(su3eps > 0.0 && su3eps < 1.0) || !std::isfinite(beta))
         return fail(c, YMFLOW_ERR_ARG, "need sweeps >= 0, hits >= 1, 0 < su3eps < 1, finite beta");
     if (start != YMFLOW_FIELD_COLD && start != YMFLOW_FIELD_HOT && start != YMFLOW_FIELD_CURRENT)
@@ -728,7 +757,8 @@ int ymflow_flow(ymflow_ctx* c, double eps, int nsteps, int measure_every, int re
 int ymflow_derivative(ymflow_ctx* c, int mu, double* z_host) {
     if (!c || !z_host || mu < 0 || mu > 3) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_derivative");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
-    if (c->slab) return fail(c, YMFLOW_ERR_STATE, "ymflow_derivative runs on a whole-lattice context, not a slab");
+    if (c->slab || c->is_block)
+        return fail(c, YMFLOW_ERR_STATE, "ymflow_derivative runs on a whole-lattice context, not a slab or block");
     DeviceGuard guard(c->device);
     int r = ensure_staging(c);
     if (r != YMFLOW_OK) return r;
@@ -870,7 +900,7 @@ extern "C" {
 int ymflow_autotune(ymflow_ctx* c, double eps, int* stage_form, int* tile_y, int* tile_z) {
     NvtxRange range("ymflow_autotune");
     if (!c || !std::isfinite(eps)) return fail(c, YMFLOW_ERR_ARG, "bad argument to ymflow_autotune");
-    if (c->slab) return fail(c, YMFLOW_ERR_ARG, "slab contexts keep the stage form of their group");
+    if (c->slab || c->is_block) return fail(c, YMFLOW_ERR_ARG, "slab and block contexts keep the stage form of their group");
     if (!c->loaded) return fail(c, YMFLOW_ERR_STATE, "no links loaded");
     DeviceGuard guard(c->device);
     YM_CK(c, cudaStreamSynchronize(c->stream), "autotune");

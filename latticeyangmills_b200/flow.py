@@ -109,6 +109,30 @@ class GluonField:
         self.sites = volume(self.size)
         return self
 
+    @classmethod
+    def block(cls, global_size: Sequence[int], origin: Sequence[int], extent: Sequence[int],
+              precision: str = "fp64", device: int = 0) -> "GluonField":
+        """Sites [origin, origin + extent) of a configuration of extents
+        global_size, with one halo layer on each side of every split direction
+        (the reference's Cartesian domain decomposition,
+        src/ParallelTools/parallel.cpp:57-100).  upload/download address the
+        block's own sites in lexicographic order over `extent`.  Flow it with
+        block_group_flow()."""
+        self = cls.__new__(cls)
+        g = tuple(int(v) for v in global_size)
+        self.global_size = g
+        self.origin = tuple(int(v) for v in origin)
+        self.size = tuple(int(v) for v in extent)
+        self.precision = precision
+        lib = N.load()
+        st = ctypes.c_int(0)
+        self._ctx = lib.ymflow_create_block(_dims(g), _dims(self.origin), _dims(self.size),
+                                            N.PRECISIONS[precision], int(device), ctypes.byref(st))
+        if not self._ctx:
+            raise N.YmflowError(st.value, lib.ymflow_last_error(None).decode(errors="replace"))
+        self.sites = volume(self.size)
+        return self
+
     def connect(self, nccl_id: bytes, rank: int, nranks: int, lower: int, upper: int) -> None:
         """Joins the NCCL communicator of nccl_id (from nccl_unique_id() on rank
         0); lower/upper are the ranks holding the neighbouring slices."""
@@ -398,6 +422,65 @@ def slab_partition(nt_global: int, nranks: int, rank: int):
     t0 = rank * base + min(rank, extra)
     nt = base + (1 if rank < extra else 0)
     return t0, nt, (rank - 1) % nranks, (rank + 1) % nranks
+
+
+def block_layout(global_size: Sequence[int], sub_size: Sequence[int]):
+    """The reference's Cartesian decomposition of a lattice into sub-lattices
+    of extents sub_size (src/ParallelTools/parallel.cpp:57-100): the grid
+    (global / sub per direction) and each block's (origin, extent), block i at
+    grid coordinates (i % grid[0], i / grid[0] % grid[1], ...), the order
+    block_group_flow takes."""
+    g = [int(v) for v in global_size]
+    s = [int(v) for v in sub_size]
+    if len(g) != 4 or len(s) != 4 or any(b < 1 or a % b for a, b in zip(g, s)):
+        raise ValueError("every sub-lattice extent must divide the lattice extent")
+    grid = [a // b for a, b in zip(g, s)]
+    blocks = []
+    for i in range(grid[0] * grid[1] * grid[2] * grid[3]):
+        c, k = [], i
+        for d in range(4):
+            c.append(k % grid[d])
+            k //= grid[d]
+        blocks.append((tuple(c[d] * s[d] for d in range(4)), tuple(s)))
+    return grid, blocks
+
+
+def block_halo_plan(grid: Sequence[int], index: int, local_size: Sequence[int]):
+    """The halo exchange of block `index` after every stage, as the library's
+    block groups run it: one phase per split direction d (grid[d] > 1) in order
+    x, y, z, t; in each, the block's first own layer (local coordinate 1)
+    goes to the lower neighbour's upper halo and its last (local_size[d] - 2)
+    to the upper neighbour's lower halo, whole faces including the halo layers
+    of the directions exchanged before.  Each entry: direction, the neighbour
+    block of each side, and the local coordinates sent and received."""
+    stride = [1, grid[0], grid[0] * grid[1], grid[0] * grid[1] * grid[2]]
+    plan = []
+    for d in range(4):
+        if grid[d] < 2:
+            continue
+        c = (index // stride[d]) % grid[d]
+        lower = index + (((c - 1) % grid[d]) - c) * stride[d]
+        upper = index + (((c + 1) % grid[d]) - c) * stride[d]
+        n = int(local_size[d])
+        plan.append({"dir": d, "lower": lower, "upper": upper,
+                     "send_to_lower": 1, "send_to_upper": n - 2, "recv_from_lower": 0, "recv_from_upper": n - 1})
+    return plan
+
+
+def block_group_flow(blocks: Sequence[GluonField], grid: Sequence[int], eps: float, nsteps: int,
+                     measure_every: int = 1, reunit_every: int = 0) -> np.ndarray:
+    """ymflow_flow over the blocks of one configuration held in this process
+    (in block_layout's order); rows (step, t, plaq, topc, energy, t2E) of the
+    whole configuration."""
+    rows = 1 + sum(1 for s in range(1, nsteps + 1)
+                   if (measure_every > 0 and s % measure_every == 0) or s == nsteps)
+    out = (N.Obs * rows)()
+    n = ctypes.c_int(0)
+    arr = (ctypes.c_void_p * len(blocks))(*[f.ctx for f in blocks])
+    N.check(N.load().ymflow_block_group_flow(arr, len(blocks), _dims(grid), float(eps), int(nsteps),
+                                             int(measure_every), int(reunit_every), out, rows, ctypes.byref(n)),
+            blocks[0].ctx)
+    return np.array([out[i].as_tuple() for i in range(n.value)])
 
 
 def slab_halo_plan(nt: int):

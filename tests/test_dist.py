@@ -178,3 +178,109 @@ def test_halo_plan_pairs_every_send_with_a_receive():
         assert {tr["to"]: tr["tag"] for tr in plan} == {"lower": 0, "upper": 1}
     with pytest.raises(ValueError):
         slab_halo_plan(0)
+
+
+# --- blocks in several directions on CPU ranks --------------------------------------
+# A 2 x 2 grid of blocks (z and t split) over four gloo ranks: each rank holds
+# its block with one halo layer in z and t, flows it stage by stage with the
+# oracle and exchanges faces on block_halo_plan's schedule (z, then t, faces
+# carrying the z halos: the edges the staples and clover need).
+BLK_N, BLK_SUB = (3, 2, 4, 6), (3, 2, 2, 3)
+
+
+def _block_rank_main(rank, world, port, q):
+    import sys
+
+    import numpy as np
+
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch
+    import torch.distributed as dist
+
+    from latticeyangmills_b200 import block_halo_plan, block_layout
+    from oracle import ymoracle as yo
+
+    dist.init_process_group("gloo")
+    n = BLK_N
+    grid, blocks = block_layout(n, BLK_SUB)
+    origin, extent = blocks[rank]
+    split = [grid[d] > 1 for d in range(4)]
+    local = [extent[d] + 2 * split[d] for d in range(4)]
+    whole = yo.gen_expiah(n, 0.4, 13)  # (t, z, y, x, 4, 18)
+    # the block with its halos, from the whole field (periodic)
+    idx = [np.array([(origin[d] - split[d] + k) % n[d] for k in range(local[d])]) for d in range(4)]
+    U = np.ascontiguousarray(whole[np.ix_(idx[3], idx[2], idx[1], idx[0])])
+    Z = np.zeros_like(U)
+
+    def layer(d, k):  # local coordinate k in direction d (numpy axis 3 - d)
+        sl = [slice(None)] * 4
+        sl[3 - d] = k
+        return tuple(sl)
+
+    plan = block_halo_plan(grid, rank, local)
+    for _ in range(3):
+        for stage in range(3):
+            yo.flow_stage(U, Z, local, 0.02, stage)
+            for ph, tr in enumerate(plan):
+                d = tr["dir"]
+                bufs, reqs = [], []
+                for side, peer, send_k, recv_k, tag in (
+                        ("lower", tr["lower"], tr["send_to_lower"], tr["recv_from_upper"], 2 * ph),
+                        ("upper", tr["upper"], tr["send_to_upper"], tr["recv_from_lower"], 2 * ph + 1)):
+                    reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(U[layer(d, send_k)])), peer,
+                                           tag=tag))
+                # what the upper neighbour sends down lands in the upper halo, and the other way round
+                for peer, recv_k, tag in ((tr["upper"], tr["recv_from_upper"], 2 * ph),
+                                          (tr["lower"], tr["recv_from_lower"], 2 * ph + 1)):
+                    buf = torch.empty(U[layer(d, recv_k)].shape, dtype=torch.float64)
+                    reqs.append(dist.irecv(buf, peer, tag=tag))
+                    bufs.append((recv_k, buf))
+                for r in reqs:
+                    r.wait()
+                for recv_k, buf in bufs:
+                    U[layer(d, recv_k)] = buf.numpy()
+    own = U[tuple(slice(split[d], split[d] + extent[d]) for d in (3, 2, 1, 0))].copy()
+    parts = [None] * world
+    dist.all_gather_object(parts, (origin, own))
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        got = np.empty_like(whole)
+        for o, part in parts:
+            got[o[3]:o[3] + part.shape[0], o[2]:o[2] + part.shape[1], o[1]:o[1] + part.shape[2],
+                o[0]:o[0] + part.shape[3]] = part
+        want = whole.copy()
+        for _ in range(3):
+            yo.flow(want, n, 0.02, 1, 0)
+        q.put(float(np.abs(got - want).max()))
+
+
+def test_block_halo_exchange_in_two_directions_reproduces_the_whole_lattice_flow():
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_block_rank_main, args=(r, 4, port, q)) for r in range(4)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+        assert p.exitcode == 0
+    assert q.get(timeout=10) == 0.0  # bit for bit
+
+
+def test_block_layout_and_plan():
+    from latticeyangmills_b200 import block_halo_plan, block_layout
+
+    grid, blocks = block_layout((8, 4, 6, 10), (4, 4, 3, 5))
+    assert grid == [2, 1, 2, 2] and len(blocks) == 8
+    assert blocks[1] == ((4, 0, 0, 0), (4, 4, 3, 5)) and blocks[2] == ((0, 0, 3, 0), (4, 4, 3, 5))
+    plan = block_halo_plan(grid, 0, (6, 4, 5, 7))
+    assert [tr["dir"] for tr in plan] == [0, 2, 3]
+    assert [(tr["lower"], tr["upper"]) for tr in plan] == [(1, 1), (2, 2), (4, 4)]
+    assert plan[2]["send_to_upper"] == 5 and plan[2]["recv_from_upper"] == 6
+    with pytest.raises(ValueError):
+        block_layout((8, 4, 6, 10), (3, 4, 3, 5))
