@@ -34,8 +34,10 @@
 // z equal to LatticeSize's, t dividing it), this driver flows each
 // configuration as that many time slabs, one per GPU (round-robin over the
 // B200s present from "Device"), with the halo exchange inside the stage kernel
-// (ymflow_slab_group_flow).  Any other SubLatticeSize is validated and the
-// lattice flows whole on one GPU.
+// (ymflow_slab_group_flow).  Any other split whose extents divide the lattice's
+// flows as blocks in the reference's Cartesian layout, one per GPU
+// round-robin (ymflow_create_block, ymflow_block_group_flow); each
+// configuration file is read once and split among the blocks on the host.
 //
 // PGFG (the reference's gauge-field generator, src/Apps/gaugefieldfactory.cpp,
 // whose update does not compile): the same App keys and validation
@@ -353,17 +355,31 @@ int main(int argc, char** argv) {
         std::printf("Total time taken: %.2fs\n", el.count());
         return 0;
     }
-    // time slabs when SubLatticeSize splits only t
-    int nslabs = 1;
-    if (in.sub[0] == in.size[0] && in.sub[1] == in.size[1] && in.sub[2] == in.size[2] && in.sub[3] < in.size[3] &&
-        in.size[3] % in.sub[3] == 0) {
-        if ((int64_t(in.size[0]) * in.size[1] * in.size[2]) % 32 == 0)
-            nslabs = in.size[3] / in.sub[3];
-        else
-            std::fprintf(stderr, "ymflow: time slabs need x y z divisible by 32; flowing the lattice whole\n");
+    // time slabs when SubLatticeSize splits only t, blocks for any other divisible split
+    int nslabs = 1, nblocks = 0;
+    int grid[4] = {1, 1, 1, 1};
+    bool divides = true, spatial_split = false;
+    for (int d = 0; d < 4; d++) {
+        divides = divides && in.sub[d] >= 1 && in.size[d] % in.sub[d] == 0;
+        if (d < 3 && in.sub[d] < in.size[d]) spatial_split = true;
     }
-    std::printf("Number of Processors: \t\t%i\n", nslabs);
-    std::printf("Number of Active Processors: \t%i\n\n", nslabs);
+    if (divides && !spatial_split && in.sub[3] < in.size[3]) {
+        if ((int64_t(in.size[0]) * in.size[1] * in.size[2]) % 32 == 0) {
+            nslabs = in.size[3] / in.sub[3];
+        } else {
+            for (int d = 0; d < 4; d++) grid[d] = in.size[d] / in.sub[d];
+            nblocks = grid[3];
+        }
+    } else if (divides && spatial_split) {
+        nblocks = 1;
+        for (int d = 0; d < 4; d++) {
+            grid[d] = in.size[d] / in.sub[d];
+            nblocks *= grid[d];
+        }
+    }
+    const int nranks = nblocks > 0 ? nblocks : nslabs;
+    std::printf("Number of Processors: \t\t%i\n", nranks);
+    std::printf("Number of Active Processors: \t%i\n\n", nranks);
 
     mkdir(in.output_dir.c_str(), 0755);
     mkdir((in.output_dir + "/flow").c_str(), 0755);
@@ -375,8 +391,22 @@ int main(int argc, char** argv) {
     }
 
     int st = 0;
-    std::vector<ymflow_ctx*> slabs;  // one context per slab (one slab: the whole lattice)
-    if (nslabs == 1) {
+    std::vector<ymflow_ctx*> slabs;  // one context per slab or block (one: the whole lattice)
+    if (nblocks > 0) {
+        int ndev = 0;
+        ymflow_device_count(&ndev);
+        for (int i = 0; i < nblocks; i++) {  // block i at grid coordinates (i % g0, i / g0 % g1, ...)
+            int origin[4], k = i;
+            for (int d = 0; d < 4; d++) {
+                origin[d] = (k % grid[d]) * in.sub[d];
+                k /= grid[d];
+            }
+            const int dev = ndev > 0 ? (in.device + i) % ndev : in.device;
+            ymflow_ctx* c = ymflow_create_block(in.size, origin, in.sub, in.precision, dev, &st);
+            if (!c) die(std::string("ymflow_create_block: ") + ymflow_last_error(nullptr));
+            slabs.push_back(c);
+        }
+    } else if (nslabs == 1) {
         ymflow_ctx* ctx = ymflow_create(in.size, in.precision, in.device, &st);
         if (!ctx) die(std::string("ymflow_create: ") + ymflow_last_error(nullptr));
         slabs.push_back(ctx);
@@ -397,12 +427,49 @@ int main(int argc, char** argv) {
     std::vector<ymflow_obs> obs(size_t(nsteps) + 2);
 
     int conf_num = 0;
+    std::vector<double> whole, part;
     for (const std::string& path : input_list(in.input_dir)) {
-        for (ymflow_ctx* c : slabs)  // each slab reads its own part of the file
-            check(ymflow_load_file(c, path.c_str(), in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0, in.chunk_sites), c,
-                  "load");
+        if (nblocks > 0) {  // the file once, each block's own sites out of it (bytes as stored)
+            const int64_t V = int64_t(in.size[0]) * in.size[1] * in.size[2] * in.size[3];
+            whole.resize(size_t(V) * 72);
+            FILE* fin = std::fopen(path.c_str(), "rb");
+            if (!fin || std::fread(whole.data(), sizeof(double), whole.size(), fin) != whole.size() ||
+                std::fgetc(fin) != EOF)
+                die("configuration file " + path + " does not hold the lattice's links");
+            std::fclose(fin);
+            const int64_t bv = int64_t(in.sub[0]) * in.sub[1] * in.sub[2] * in.sub[3];
+            part.resize(size_t(bv) * 72);
+            for (int i = 0; i < nblocks; i++) {
+                int origin[4], k = i;
+                for (int d = 0; d < 4; d++) {
+                    origin[d] = (k % grid[d]) * in.sub[d];
+                    k /= grid[d];
+                }
+                size_t o = 0;
+                for (int t = 0; t < in.sub[3]; t++)
+                    for (int z = 0; z < in.sub[2]; z++)
+                        for (int y = 0; y < in.sub[1]; y++) {  // one run of x per (t, z, y)
+                            const int64_t s0 =
+                                origin[0] + int64_t(in.size[0]) *
+                                                (origin[1] + y + int64_t(in.size[1]) *
+                                                                     (origin[2] + z + int64_t(in.size[2]) * (origin[3] + t)));
+                            std::memcpy(part.data() + o, whole.data() + s0 * 72, size_t(in.sub[0]) * 72 * sizeof(double));
+                            o += size_t(in.sub[0]) * 72;
+                        }
+                check(ymflow_upload_sites(slabs[i], part.data(), 0, bv, in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0),
+                      slabs[i], "upload");
+            }
+        } else {
+            for (ymflow_ctx* c : slabs)  // each slab reads its own part of the file
+                check(ymflow_load_file(c, path.c_str(), in.big_endian ? YMFLOW_IO_BIG_ENDIAN : 0, in.chunk_sites), c,
+                      "load");
+        }
         int n_out = 0;
-        if (nslabs == 1)
+        if (nblocks > 0)
+            check(ymflow_block_group_flow(slabs.data(), nblocks, grid, in.epsilon, nsteps, 1, in.reunit_every,
+                                          obs.data(), int(obs.size()), &n_out),
+                  ctx, "flow");
+        else if (nslabs == 1)
             check(ymflow_flow(ctx, in.epsilon, nsteps, 1, in.reunit_every, obs.data(), int(obs.size()), &n_out), ctx,
                   "flow");
         else

@@ -92,6 +92,25 @@ def test_flow_app_time_slabs_from_sublattice_size(tmp_path):
         assert (tmp_path / "out" / f).read_bytes() == (ex / f).read_bytes(), f
 
 
+@pytest.mark.parametrize("sub,nblocks", [({"x": 2, "y": 4, "z": 2, "t": 2}, 8), ({"x": 4, "y": 2, "z": 4, "t": 4}, 2),
+                                         ({"x": 2, "y": 2, "z": 2, "t": 2}, 16)])
+def test_flow_app_blocks_from_sublattice_size(tmp_path, sub, nblocks):
+    """A SubLatticeSize that splits x, y or z flows each configuration as blocks
+    in the reference's Cartesian layout (parallel.cpp:57-100): the same files as
+    the reference application, its terminal lines apart from the processor
+    count."""
+    run = prepare(tmp_path, {"SubLatticeSize": sub})
+    res = subprocess.run([str(APP), str(run)], capture_output=True, text=True, check=True)
+    got = [l for l in res.stdout.splitlines(keepends=True) if not l.startswith("Total time taken")]
+    exp = (GOLDEN / "app_flow" / "expected" / "stdout.txt").read_text().splitlines(keepends=True)
+    assert "Number of Processors: \t\t%d\n" % nblocks in got
+    keep = lambda lines: [l for l in lines if not l.startswith(("Number of", "Sublattice Size"))]
+    assert keep(got) == keep(exp)
+    ex = GOLDEN / "app_flow" / "expected"
+    for f in ["observables.dat", "flow/conf0000.dat", "flow/conf0001.dat"]:
+        assert (tmp_path / "out" / f).read_bytes() == (ex / f).read_bytes(), f
+
+
 def test_flow_app_empty_input_dir(tmp_path):
     """No .bin files: the reference writes its headers and flows nothing."""
     run = prepare(tmp_path)
