@@ -149,12 +149,82 @@ __global__ void __launch_bounds__(128, SplitMinBlocks<F>::value)
     split_link_update<F, STAGE>(in, out, zf, hf, g, eps, s, mu);
 }
 
+// The same two kernels with the work list as a launch parameter (up to
+// kParamConfs configurations): the binary search and every geometry read of
+// the link code come from the constant bank instead of global memory, as a
+// single configuration's Geo does.  The plaquette-field kernel takes two
+// planes per thread (64 sites per block), as the single-configuration one.
+constexpr int kParamConfs = 128;
+struct EnsTable {
+    EnsConf c[kParamConfs];
+    int n;
+};
+
+__device__ __forceinline__ int find_conf_param(const EnsTable& t, int item) {
+    int lo = 0, hi = t.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t.c[mid].blk0 <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class F>
+__global__ void __launch_bounds__(192) ens_plaq_param_kernel(char* u, char* h, const __grid_constant__ EnsTable tab) {
+    const int w = int(threadIdx.x >> 5);
+    const int item = int(blockIdx.x) * 2 + w / 3;
+    if (item >= tab.c[tab.n - 1].blk0 + tab.c[tab.n - 1].nblk) return;
+    const EnsConf& C = tab.c[find_conf_param(tab, item)];
+    const Geo& g = C.g;
+    const int s = (item - C.blk0) * 32 + int(threadIdx.x & 31);
+    if (s >= g.V) return;
+    const F uf{u + C.uoff, g.V};
+    const ForceField<typename F::Real> hf{h + C.hoff, g.V};
+    const int pr = w % 3;
+    const int p0 = pr == 0 ? 0 : (pr == 1 ? 2 : 3);
+    const int p1 = pr == 0 ? 1 : (pr == 1 ? 4 : 5);
+    int c[4];
+    g.coords(s, c);
+    hf.store(p0, s, plane_generator(uf, g, s, c, plane_a(p0), plane_b(p0)));
+    hf.store(p1, s, plane_generator(uf, g, s, c, plane_a(p1), plane_b(p1)));
+}
+
+template <class F, int STAGE>
+__global__ void __launch_bounds__(128, SplitMinBlocks<F>::value)
+    ens_split_param_kernel(char* uin, char* uout, char* z, char* h, const __grid_constant__ EnsTable tab,
+                           typename F::Real eps) {
+    using R = typename F::Real;
+    const int mu = int(threadIdx.x >> 5) & 3;
+    const int item = blockIdx.x;
+    const EnsConf& C = tab.c[find_conf_param(tab, item)];
+    const Geo& g = C.g;
+    const int s = (item - C.blk0) * 32 + int(threadIdx.x & 31);
+    if (s >= g.V) return;
+    const F in{uin + C.uoff, g.V}, out{uout + C.uoff, g.V};
+    const ForceField<R> zf{z + C.zoff, g.V}, hf{h + C.hoff, g.V};
+    split_link_update<F, STAGE>(in, out, zf, hf, g, eps, s, mu);
+}
+
 template <class F>
 static cudaError_t launch_ens_split_typed(int stage, void* uin, void* uout, void* z, void* h, const EnsConf* confs,
-                                          int nconf, int nitems, double eps, cudaStream_t st) {
+                                          int nconf, int nitems, double eps, cudaStream_t st,
+                                          const EnsConf* host_confs) {
     using R = typename F::Real;
     const R e = R(stage == 0 ? eps * 0.25 : eps);
     char *a = (char*)uin, *b = (char*)uout, *zz = (char*)z, *hh = (char*)h;
+    if (host_confs && nconf <= kParamConfs) {
+        EnsTable tab;
+        std::memcpy(tab.c, host_confs, sizeof(EnsConf) * size_t(nconf));
+        tab.n = nconf;
+        ens_plaq_param_kernel<F><<<(nitems + 1) / 2, 192, 0, st>>>(a, hh, tab);
+        switch (stage) {
+            case 0: ens_split_param_kernel<F, 0><<<nitems, 128, 0, st>>>(a, b, zz, hh, tab, e); break;
+            case 1: ens_split_param_kernel<F, 1><<<nitems, 128, 0, st>>>(a, b, zz, hh, tab, e); break;
+            default: ens_split_param_kernel<F, 2><<<nitems, 128, 0, st>>>(a, b, zz, hh, tab, e); break;
+        }
+        return cudaGetLastError();
+    }
     ens_plaq_kernel<F><<<nitems, 192, 0, st>>>(a, hh, confs, nconf);
     switch (stage) {
         case 0: ens_split_kernel<F, 0><<<nitems, 128, 0, st>>>(a, b, zz, hh, confs, nconf, e); break;
@@ -274,11 +344,12 @@ cudaError_t launch_ens_tile_stage(int prec, int stage, void* uin, void* uout, vo
 
 // Work items must be 32-site groups (block 128).
 cudaError_t launch_ens_split_stage(int prec, int stage, void* uin, void* uout, void* z, void* h, const EnsConf* confs,
-                                   int nconf, int nitems, double eps, cudaStream_t st) {
+                                   int nconf, int nitems, double eps, cudaStream_t st,
+                                   const EnsConf* host_confs = nullptr) {
     switch (prec) {
-        case kFP64: return launch_ens_split_typed<FieldD18>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st);
-        case kFP32_18: return launch_ens_split_typed<FieldF18>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st);
-        case kFP32_12: return launch_ens_split_typed<FieldF12>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st);
+        case kFP64: return launch_ens_split_typed<FieldD18>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st, host_confs);
+        case kFP32_18: return launch_ens_split_typed<FieldF18>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st, host_confs);
+        case kFP32_12: return launch_ens_split_typed<FieldF12>(stage, uin, uout, z, h, confs, nconf, nitems, eps, st, host_confs);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -462,7 +533,7 @@ cudaError_t enqueue_ens_step(ymflow_ens* e, int from, double eps) {
                                                         e->nunits, e->tile_grid, e->tile_threads, e->tile_smem, eps,
                                                         e->stream)
                         : e->split ? launch_ens_split_stage(e->prec, s, in[s], out[s], e->z, e->h, e->confs_dev,
-                                                            e->nconf, ni, eps, e->stream)
+                                                            e->nconf, ni, eps, e->stream, e->confs.data())
                                    : launch_ens_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf, ni,
                                                       grid, e->block, eps, e->stream);
         if (r != cudaSuccess) return r;
@@ -560,7 +631,8 @@ float time_stage0(ymflow_ens* e, double eps, int reps) {
             return launch_ens_tile_stage(e->prec, 0, a, b, e->z, e->confs_dev, e->nconf, e->nunits, e->tile_grid,
                                          e->tile_threads, e->tile_smem, eps, e->stream);
         if (e->split)
-            return launch_ens_split_stage(e->prec, 0, a, b, e->z, e->h, e->confs_dev, e->nconf, ni, eps, e->stream);
+            return launch_ens_split_stage(e->prec, 0, a, b, e->z, e->h, e->confs_dev, e->nconf, ni, eps, e->stream,
+                                          e->confs.data());
         return launch_ens_stage(e->prec, 0, a, b, e->z, e->confs_dev, e->nconf, ni, grid, e->block, eps, e->stream);
     };
     if (launch() != cudaSuccess) return -1.f;
