@@ -868,13 +868,7 @@ int time_stage0(ymflow_ctx* c, double eps, int reps, float* ms) {
     const void* a = c->u[c->cur];
     void* b = c->u[1 - c->cur];
     auto launch = [&]() -> cudaError_t {
-        if (c->stage_form == 1) {
-            cudaError_t e = launch_plaq_field(c->prec, a, c->hfield, c->geo, c->stream);
-            if (e != cudaSuccess) return e;
-            return launch_rk_split_stage(c->prec, 0, a, b, c->z, c->hfield, c->geo, eps, c->stream);
-        }
-        if (c->stage_form == 2) return launch_rk_tile_stage(c->prec, 0, a, b, c->z, c->geo, c->tile, eps, c->stream);
-        return launch_rk_stage(c->prec, 0, a, b, c->z, c->geo, eps, c->block, c->stream);
+        return enqueue_stage(c, 0, a, b, eps);
     };
     for (int i = 0; i < 2; i++) YM_CK(c, launch(), "autotune warm-up");
     YM_CK(c, cudaEventRecord(c->ev0, c->stream), "event record");
