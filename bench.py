@@ -353,6 +353,7 @@ def ensemble_measure(prec: str, steps: int, dev: int):
     for c in range(len(sizes)):
         ens.init_links(c, "expiah", float(a_list[c]), SEED + c, c)
     block, grid = ens.autotune(EPS)
+    form = ens.tuning()[0]
     ens.time_steps(EPS, 3)
     ms = ens.time_steps(EPS, steps)
     ens.close()
@@ -367,7 +368,8 @@ def ensemble_measure(prec: str, steps: int, dev: int):
     return {"configs": len(sizes), "sizes": "16x8^4 + 16x12^4 + 16x16^4 + 16x16^3x32", "precision": prec,
             "steps": steps, "link_updates_per_s": links * steps / (ms / 1e3),
             "one_by_one_link_updates_per_s": links * steps / (one_ms / 1e3),
-            "speedup_vs_one_by_one": one_ms / ms, "autotuned": {"block": block, "grid": grid}}
+            "speedup_vs_one_by_one": one_ms / ms,
+            "autotuned": {"stage_form": form, "block": block, "grid": grid}}
 
 
 def workload_run(args, dev: int):

@@ -31,6 +31,7 @@ IO_BIG_ENDIAN = 1
 NCCL_ID_BYTES = 128
 OPT_BLOCK, OPT_GRAPH, OPT_OBS_BLOCK, OPT_STAGE_FORM, OPT_TILE, OPT_TIMED_REUNIT = 1, 2, 3, 4, 5, 6
 STAGE_FUSED, STAGE_SPLIT, STAGE_TILE = 0, 1, 2
+ENS_SPLIT_RUNS = 3  # ensembles: the two-kernel stage per run of equal extents
 
 # every symbol include/ymflow.h declares
 EXPORTS = (

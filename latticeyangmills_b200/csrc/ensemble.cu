@@ -234,6 +234,87 @@ static cudaError_t launch_ens_split_typed(int stage, void* uin, void* uout, void
     return cudaGetLastError();
 }
 
+// The same two kernels per run of consecutive configurations of one geometry
+// (EnsRun): the run's work items are its (configuration, 32-site group) pairs,
+// configuration-major, and the geometry is a launch parameter read at fixed
+// constant-bank offsets, exactly as the single-configuration kernels read
+// their Geo; a block finds its configuration by one division.  A stage is
+// one plaquette-field launch and one stage launch per run.
+struct EnsRun {
+    Geo g;
+    int nconf;                          // configurations in the run
+    int nblk;                           // 32-site groups per configuration
+    int64_t ustride, zstride, hstride;  // bytes from one configuration to the next in each pool
+};
+
+template <class F>
+__global__ void __launch_bounds__(192) ens_run_plaq_kernel(char* u, char* h, const __grid_constant__ EnsRun r) {
+    const int w = int(threadIdx.x >> 5);
+    const int item = int(blockIdx.x) * 2 + w / 3;
+    const int conf = item / r.nblk;
+    if (conf >= r.nconf) return;
+    const Geo& g = r.g;
+    const int s = (item - conf * r.nblk) * 32 + int(threadIdx.x & 31);
+    if (s >= g.V) return;
+    const F uf{u + conf * r.ustride, g.V};
+    const ForceField<typename F::Real> hf{h + conf * r.hstride, g.V};
+    const int pr = w % 3;
+    const int p0 = pr == 0 ? 0 : (pr == 1 ? 2 : 3);
+    const int p1 = pr == 0 ? 1 : (pr == 1 ? 4 : 5);
+    int c[4];
+    g.coords(s, c);
+    hf.store(p0, s, plane_generator(uf, g, s, c, plane_a(p0), plane_b(p0)));
+    hf.store(p1, s, plane_generator(uf, g, s, c, plane_a(p1), plane_b(p1)));
+}
+
+template <class F, int STAGE>
+__global__ void __launch_bounds__(128, SplitMinBlocks<F>::value)
+    ens_run_split_kernel(char* uin, char* uout, char* z, char* h, const __grid_constant__ EnsRun r,
+                         typename F::Real eps) {
+    using R = typename F::Real;
+    const int mu = int(threadIdx.x >> 5) & 3;
+    const int item = int(blockIdx.x);
+    const int conf = item / r.nblk;
+    const Geo& g = r.g;
+    const int s = (item - conf * r.nblk) * 32 + int(threadIdx.x & 31);
+    if (s >= g.V) return;
+    const F in{uin + conf * r.ustride, g.V}, out{uout + conf * r.ustride, g.V};
+    const ForceField<R> zf{z + conf * r.zstride, g.V}, hf{h + conf * r.hstride, g.V};
+    split_link_update<F, STAGE>(in, out, zf, hf, g, eps, s, mu);
+}
+
+// A run and where its first configuration starts in each pool.
+struct EnsRunLaunch {
+    EnsRun r;
+    int64_t uoff, zoff, hoff;
+};
+
+// One stage of one run: its plaquette-field launch, then its stage launch.
+template <class F>
+static cudaError_t launch_ens_run_typed(int stage, void* uin, void* uout, void* z, void* h, const EnsRunLaunch& L,
+                                        double eps, cudaStream_t st) {
+    using R = typename F::Real;
+    const R e = R(stage == 0 ? eps * 0.25 : eps);
+    const int items = L.r.nconf * L.r.nblk;
+    char *a = (char*)uin + L.uoff, *b = (char*)uout + L.uoff, *zz = (char*)z + L.zoff, *hh = (char*)h + L.hoff;
+    ens_run_plaq_kernel<F><<<(items + 1) / 2, 192, 0, st>>>(a, hh, L.r);
+    switch (stage) {
+        case 0: ens_run_split_kernel<F, 0><<<items, 128, 0, st>>>(a, b, zz, hh, L.r, e); break;
+        case 1: ens_run_split_kernel<F, 1><<<items, 128, 0, st>>>(a, b, zz, hh, L.r, e); break;
+        default: ens_run_split_kernel<F, 2><<<items, 128, 0, st>>>(a, b, zz, hh, L.r, e); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ens_run_stage(int prec, int stage, void* uin, void* uout, void* z, void* h, const EnsRunLaunch& L,
+                                 double eps, cudaStream_t st) {
+    switch (prec) {
+        case kFP32_18: return launch_ens_run_typed<FieldF18>(stage, uin, uout, z, h, L, eps, st);
+        case kFP32_12: return launch_ens_run_typed<FieldF12>(stage, uin, uout, z, h, L, eps, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 // The one-kernel stage with a tile's plaquette field in shared memory
 // (flow_tile.cuh) over every configuration at once: the unit lists of all
 // configurations, concatenated, are split into contiguous runs, one per
@@ -402,6 +483,14 @@ struct ymflow_ens {
     void* z = nullptr;
     void* h = nullptr;       // plane generators of the two-kernel stage (FP32 ensembles)
     bool split = false;      // FP32: the two-kernel stage, one block per work item
+    bool by_runs = false;    // ... launched per run of equal-geometry configurations
+    std::vector<EnsRunLaunch> runs;
+    // the runs' launch streams (run i on side[i % side.size()]): each run's
+    // stages depend only on its own earlier stages, so the runs flow
+    // concurrently, as parallel branches of the step graph
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> side_done;
+    cudaEvent_t fork = nullptr;
     bool tile = false;       // the one-kernel stage with tiles in shared memory (over split / fused)
     int tile_threads = 0;    // its block size: every configuration's tile has at most this many sites
     int tile_grid = 0;       // its persistent blocks
@@ -521,6 +610,33 @@ int nitems(const ymflow_ens* e) {
     return e->confs.empty() ? 0 : e->confs.back().blk0 + e->confs.back().nblk;
 }
 
+// Stages [0, nst) of every run, in[s] -> out[s]: forked from the ensemble's
+// stream onto the side streams and joined back (parallel branches when
+// captured into the step graph).  With one side stream, everything stays on
+// the ensemble's stream.
+cudaError_t enqueue_runs(ymflow_ens* e, int nst, void* const* in, void* const* out, double eps) {
+    const int ns = int(e->side.size());
+    if (ns == 0) {
+        for (int s = 0; s < nst; s++)
+            for (const EnsRunLaunch& L : e->runs) {
+                const cudaError_t r = launch_ens_run_stage(e->prec, s, in[s], out[s], e->z, e->h, L, eps, e->stream);
+                if (r != cudaSuccess) return r;
+            }
+        return cudaSuccess;
+    }
+    cudaError_t r = cudaEventRecord(e->fork, e->stream);
+    for (int k = 0; k < ns && r == cudaSuccess; k++) r = cudaStreamWaitEvent(e->side[k], e->fork, 0);
+    for (int s = 0; s < nst && r == cudaSuccess; s++)
+        for (size_t i = 0; i < e->runs.size() && r == cudaSuccess; i++)
+            r = launch_ens_run_stage(e->prec, s, in[s], out[s], e->z, e->h, e->runs[i], eps, e->side[i % ns]);
+    for (int k = 0; k < ns; k++) {  // join every branch, also after a failed launch
+        const cudaError_t j = cudaEventRecord(e->side_done[k], e->side[k]);
+        const cudaError_t w = j == cudaSuccess ? cudaStreamWaitEvent(e->stream, e->side_done[k], 0) : j;
+        if (r == cudaSuccess) r = w;
+    }
+    return r;
+}
+
 cudaError_t enqueue_ens_step(ymflow_ens* e, int from, double eps) {
     void* a = e->u[from];
     void* b = e->u[1 - from];
@@ -528,6 +644,7 @@ cudaError_t enqueue_ens_step(ymflow_ens* e, int from, double eps) {
     void* out[3] = {b, a, b};
     const int ni = nitems(e);
     const int grid = e->grid > 0 ? std::min(e->grid, ni) : ni;
+    if (!e->tile && e->split && e->by_runs) return enqueue_runs(e, 3, in, out, eps);
     for (int s = 0; s < 3; s++) {
         cudaError_t r = e->tile ? launch_ens_tile_stage(e->prec, s, in[s], out[s], e->z, e->confs_dev, e->nconf,
                                                         e->nunits, e->tile_grid, e->tile_threads, e->tile_smem, eps,
@@ -630,6 +747,7 @@ float time_stage0(ymflow_ens* e, double eps, int reps) {
         if (e->tile)
             return launch_ens_tile_stage(e->prec, 0, a, b, e->z, e->confs_dev, e->nconf, e->nunits, e->tile_grid,
                                          e->tile_threads, e->tile_smem, eps, e->stream);
+        if (e->split && e->by_runs) return enqueue_runs(e, 1, &a, &b, eps);
         if (e->split)
             return launch_ens_split_stage(e->prec, 0, a, b, e->z, e->h, e->confs_dev, e->nconf, ni, eps, e->stream,
                                           e->confs.data());
@@ -719,6 +837,43 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
     // FP32 ensembles flow with the two-kernel stage, as FP32 single contexts do
     e->split = precision != YMFLOW_FP64;
     if (r == YMFLOW_OK && e->split) r = ens_alloc(e, &e->h, size_t(ho), "plane-generator pool");
+    for (int c = 0; c < nconf; c++) {  // runs of consecutive configurations with equal extents
+        const EnsConf& C = e->confs[c];
+        if (c > 0 && std::equal(C.g.n, C.g.n + 4, e->confs[c - 1].g.n)) {
+            e->runs.back().r.nconf++;
+            continue;
+        }
+        EnsRunLaunch L;
+        L.r.g = C.g;
+        L.r.nconf = 1;
+        L.r.nblk = (C.g.V + 31) / 32;
+        L.r.ustride = int64_t(link_field_bytes(e->prec, C.g.V));
+        L.r.zstride = int64_t(force_field_bytes(e->prec, C.g.V));
+        L.r.hstride = int64_t(plane_field_bytes(e->prec, C.g.V));
+        L.uoff = C.uoff;
+        L.zoff = C.zoff;
+        L.hoff = C.hoff;
+        e->runs.push_back(L);
+    }
+    if (r == YMFLOW_OK && e->split && e->runs.size() > 1) {  // up to four concurrent branches
+        const size_t ns = std::min<size_t>(e->runs.size(), 4);
+        if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) r = YMFLOW_ERR_CUDA;
+        for (size_t k = 0; k < ns && r == YMFLOW_OK; k++) {
+            cudaStream_t st = nullptr;
+            cudaEvent_t ev = nullptr;
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+                r = YMFLOW_ERR_CUDA;
+                break;
+            }
+            e->side.push_back(st);
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+                r = YMFLOW_ERR_CUDA;
+                break;
+            }
+            e->side_done.push_back(ev);
+        }
+        if (r == YMFLOW_OK && e->side_done.size() != e->side.size()) r = YMFLOW_ERR_CUDA;
+    }
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->confs_dev, sizeof(EnsConf) * nconf, "work list");
     if (r == YMFLOW_OK) r = ens_alloc(e, (void**)&e->deviation, sizeof(unsigned long long), "drift flag");
     if (r == YMFLOW_OK) {
@@ -740,6 +895,7 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
         auto it = g_tune_cache.find(e->signature);
         if (it != g_tune_cache.end()) {
             const EnsTuning tn = it->second;
+            e->by_runs = tn.form == 3;
             if (tn.form == 2 && set_tiles(e, tn.block)) {
                 e->tile = true;
             } else {
@@ -767,6 +923,9 @@ void ymflow_ensemble_destroy(ymflow_ens* e) {
                     (void*)e->meas, (void*)e->deviation})
         if (p) cudaFree(p);
     if (e->meas_host) cudaFreeHost(e->meas_host);
+    for (cudaStream_t st : e->side) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : e->side_done) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -929,6 +1088,7 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     std::vector<EnsTuning> cands;
     if (e->split) {
         cands.push_back({1, 128, 0});
+        cands.push_back({3, 128, 0});
     } else {
         const int resident = ens_max_resident(e->prec, 128);
         for (int grid : {0, resident * sms, 2 * resident * sms}) cands.push_back({0, 128, grid});
@@ -939,6 +1099,7 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     EnsTuning pick = cands.front();
     for (const EnsTuning& ch : cands) {
         e->tile = false;
+        e->by_runs = ch.form == 3;
         if (ch.form == 2) {
             if (!set_tiles(e, ch.block)) continue;
             e->tile = true;
@@ -956,6 +1117,7 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     }
     e->tile = false;
     e->split = was_split;
+    e->by_runs = pick.form == 3;
     if (pick.form == 2 && set_tiles(e, pick.block)) {
         e->tile = true;
     } else {
@@ -982,17 +1144,19 @@ int ymflow_ensemble_set_tuning(ymflow_ens* e, int stage_form, int block, int gri
             return efail(e, YMFLOW_ERR_ARG, "no tiling of every configuration within " + std::to_string(block) +
                                                 " threads and 227 KB of shared memory");
         e->tile = true;
-    } else if (stage_form == 0 || (stage_form == 1 && e->h)) {
-        if (stage_form == 1 && block != 128) return efail(e, YMFLOW_ERR_ARG, "the two-kernel stage runs 128 threads");
+        e->by_runs = false;
+    } else if (stage_form == 0 || ((stage_form == 1 || stage_form == 3) && e->h)) {
+        if (stage_form != 0 && block != 128) return efail(e, YMFLOW_ERR_ARG, "the two-kernel stage runs 128 threads");
         if (block != 128) return efail(e, YMFLOW_ERR_ARG, "the per-link kernel runs 128 threads");
         if (grid < 0) return efail(e, YMFLOW_ERR_ARG, "grid < 0");
         e->tile = false;
-        e->split = stage_form == 1;
-        e->grid = stage_form == 1 ? 0 : grid;
+        e->split = stage_form == 1 || stage_form == 3;
+        e->by_runs = stage_form == 3;
+        e->grid = stage_form == 0 ? grid : 0;
         const int r = set_block(e, 128);
         if (r != YMFLOW_OK) return r;
     } else {
-        return efail(e, YMFLOW_ERR_ARG, "stage form is 0, 1 (FP32 ensembles) or 2");
+        return efail(e, YMFLOW_ERR_ARG, "stage form is 0, 1 or 3 (FP32 ensembles) or 2");
     }
     YE_CK(e, cudaStreamSynchronize(e->stream), "set tuning");
     drop_graphs(e);
@@ -1001,7 +1165,7 @@ int ymflow_ensemble_set_tuning(ymflow_ens* e, int stage_form, int block, int gri
 
 int ymflow_ensemble_tuning(const ymflow_ens* e, int* stage_form, int* block, int* grid) {
     if (!e) return YMFLOW_ERR_ARG;
-    if (stage_form) *stage_form = e->tile ? 2 : (e->split ? 1 : 0);
+    if (stage_form) *stage_form = e->tile ? 2 : (e->split ? (e->by_runs ? 3 : 1) : 0);
     if (block) *block = e->tile ? e->tile_threads : e->block;
     if (grid) *grid = e->tile ? e->tile_grid : e->grid;
     return YMFLOW_OK;

@@ -116,3 +116,34 @@ def test_set_tuning_refusals():
     with Ensemble([(8, 8, 8, 8)], "fp64") as ens:
         with pytest.raises(YmflowError):
             ens.set_tuning(1)  # no plane-generator pool in FP64 ensembles
+
+
+# runs of equal extents: two of 8^4, one of 3x4x5x6, three of 6^3x8, one of 8^4
+RUN_SIZES = [(8, 8, 8, 8)] * 2 + [(3, 4, 5, 6)] + [(6, 6, 6, 8)] * 3 + [(8, 8, 8, 8)]
+
+
+@pytest.mark.parametrize("prec", ["fp32_18", "fp32_12"])
+def test_per_run_two_kernel_stage_equals_work_list_form(prec):
+    """Stage form 3 (the two-kernel stage launched per run of equal extents,
+    the runs as concurrent branches of the step graph) runs the same link code
+    as form 1 over the work list: rows and links bit for bit, with the
+    reunitarisation between steps."""
+    from latticeyangmills_b200 import Ensemble
+
+    out = {}
+    for form in (1, 3):
+        with Ensemble(RUN_SIZES, prec) as ens:
+            ens.set_tuning(form)
+            assert ens.tuning() == (form, 128, 0)
+            for c in range(len(RUN_SIZES)):
+                ens.init_links(c, "expiah", 0.3 + 0.02 * c, 20 + c)
+            rows = ens.flow(0.02, 6, 3, reunit_every=2)
+            out[form] = (rows, [ens.download(c) for c in range(len(RUN_SIZES))])
+    np.testing.assert_array_equal(out[3][0], out[1][0])
+    for a, b in zip(out[3][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
+    with Ensemble([(8, 8, 8, 8)], "fp64") as ens:
+        from latticeyangmills_b200 import YmflowError
+
+        with pytest.raises(YmflowError):
+            ens.set_tuning(3)  # FP64 ensembles have no plane-generator pool
