@@ -186,8 +186,11 @@ __global__ void __launch_bounds__(192) ens_plaq_param_kernel(char* u, char* h, c
     const int p1 = pr == 0 ? 1 : (pr == 1 ? 4 : 5);
     int c[4];
     g.coords(s, c);
-    hf.store(p0, s, plane_generator(uf, g, s, c, plane_a(p0), plane_b(p0)));
-    hf.store(p1, s, plane_generator(uf, g, s, c, plane_a(p1), plane_b(p1)));
+    // both planes before either store: the link the two share is loaded once
+    const auto h0 = plane_generator(uf, g, s, c, plane_a(p0), plane_b(p0));
+    const auto h1 = plane_generator(uf, g, s, c, plane_a(p1), plane_b(p1));
+    hf.store(p0, s, h0);
+    hf.store(p1, s, h1);
 }
 
 template <class F, int STAGE>
@@ -263,8 +266,11 @@ __global__ void __launch_bounds__(192) ens_run_plaq_kernel(char* u, char* h, con
     const int p1 = pr == 0 ? 1 : (pr == 1 ? 4 : 5);
     int c[4];
     g.coords(s, c);
-    hf.store(p0, s, plane_generator(uf, g, s, c, plane_a(p0), plane_b(p0)));
-    hf.store(p1, s, plane_generator(uf, g, s, c, plane_a(p1), plane_b(p1)));
+    // both planes before either store: the link the two share is loaded once
+    const auto h0 = plane_generator(uf, g, s, c, plane_a(p0), plane_b(p0));
+    const auto h1 = plane_generator(uf, g, s, c, plane_a(p1), plane_b(p1));
+    hf.store(p0, s, h0);
+    hf.store(p1, s, h1);
 }
 
 template <class F, int STAGE>
@@ -610,6 +616,19 @@ int nitems(const ymflow_ens* e) {
     return e->confs.empty() ? 0 : e->confs.back().blk0 + e->confs.back().nblk;
 }
 
+// Puts the ensemble into a tuning's form; a tiling that no longer fits falls
+// back to one 128-thread block per work item.
+int apply_tuning(ymflow_ens* e, const EnsTuning& tn) {
+    e->by_runs = tn.form == 3;
+    if (tn.form == 2 && set_tiles(e, tn.block)) {
+        e->tile = true;
+        return YMFLOW_OK;
+    }
+    e->tile = false;
+    e->grid = tn.form == 2 ? 0 : tn.grid;
+    return set_block(e, tn.form == 2 ? 128 : tn.block);
+}
+
 // Stages [0, nst) of every run, in[s] -> out[s]: forked from the ensemble's
 // stream onto the side streams and joined back (parallel branches when
 // captured into the step graph).  With one side stream, everything stays on
@@ -894,14 +913,7 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(e->signature);
         if (it != g_tune_cache.end()) {
-            const EnsTuning tn = it->second;
-            e->by_runs = tn.form == 3;
-            if (tn.form == 2 && set_tiles(e, tn.block)) {
-                e->tile = true;
-            } else {
-                e->grid = tn.form == 2 ? 0 : tn.grid;
-                r = set_block(e, tn.form == 2 ? 128 : tn.block);
-            }
+            r = apply_tuning(e, it->second);
             e->tuned = true;
         }
     }
@@ -1080,6 +1092,28 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     for (int c = 0; c < e->nconf; c++)
         if (!e->loaded[c]) return efail(e, YMFLOW_ERR_STATE, "configuration not loaded");
     DeviceGuard guard(e->device);
+    auto report = [&]() {
+        if (block_out) *block_out = e->tile ? e->tile_threads : e->block;
+        if (grid_out) *grid_out = e->tile ? e->tile_grid : e->grid;
+    };
+    bool cached = false;
+    EnsTuning tn{};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(e->signature);
+        if (it != g_tune_cache.end()) {
+            cached = true;
+            tn = it->second;
+        }
+    }
+    if (cached) {  // an ensemble of the same sizes and precision was tuned in this process
+        const int r = apply_tuning(e, tn);
+        if (r != YMFLOW_OK) return r;
+        drop_graphs(e);
+        e->tuned = true;
+        report();
+        return YMFLOW_OK;
+    }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
     // candidates: the per-link kernel over {one block per item, 1x and 2x the
@@ -1115,24 +1149,16 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
             pick = ch;
         }
     }
-    e->tile = false;
     e->split = was_split;
-    e->by_runs = pick.form == 3;
-    if (pick.form == 2 && set_tiles(e, pick.block)) {
-        e->tile = true;
-    } else {
-        e->grid = pick.form == 2 ? 0 : pick.grid;
-        int r = set_block(e, pick.form == 2 ? 128 : pick.block);
-        if (r != YMFLOW_OK) return r;
-    }
+    const int r = apply_tuning(e, pick);
+    if (r != YMFLOW_OK) return r;
     drop_graphs(e);
     e->tuned = true;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune_cache[e->signature] = pick;
     }
-    if (block_out) *block_out = e->tile ? e->tile_threads : e->block;
-    if (grid_out) *grid_out = e->tile ? e->tile_grid : e->grid;
+    report();
     return YMFLOW_OK;
 }
 

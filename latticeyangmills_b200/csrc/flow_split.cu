@@ -26,10 +26,10 @@ namespace ym {
 
 // One thread per (site, pair of planes): six warps cover 64 sites, warps
 // 3k .. 3k + 2 the planes {(0,1), (0,2)}, {(0,3), (1,3)}, {(1,2), (2,3)} of
-// site group k (the two planes of a pair share one of the site's links).  The
-// second plane's loads issue during the first plane's products: against one
-// plane per thread, the FP32-18 kernel runs 16 % faster at 32^4 on B200 (0.180
-// -> 0.151 ms), the 12-real one 1.6 % (0.148 -> 0.146).
+// site group k (the two planes of a pair share one of the site's links,
+// loaded once).  The second plane's loads issue during the first plane's
+// products: against one plane per thread, the FP32-18 kernel ran 16 % faster
+// at 32^4 on B200 (0.180 -> 0.151 ms), the 12-real one 1.6 % (0.148 -> 0.146).
 template <class F>
 __global__ void __launch_bounds__(192) plaq_field_kernel(F u, ForceField<typename F::Real> hf, Geo g) {
     const int w = int(threadIdx.x >> 5);
@@ -40,8 +40,11 @@ __global__ void __launch_bounds__(192) plaq_field_kernel(F u, ForceField<typenam
     const int p1 = pr == 0 ? 1 : (pr == 1 ? 4 : 5);
     int c[4];
     g.coords(s, c);
-    hf.store(p0, s, plane_generator(u, g, s, c, plane_a(p0), plane_b(p0)));
-    hf.store(p1, s, plane_generator(u, g, s, c, plane_a(p1), plane_b(p1)));
+    // both planes before either store: the link the two share is loaded once
+    const auto h0 = plane_generator(u, g, s, c, plane_a(p0), plane_b(p0));
+    const auto h1 = plane_generator(u, g, s, c, plane_a(p1), plane_b(p1));
+    hf.store(p0, s, h0);
+    hf.store(p1, s, h1);
 }
 
 // One thread per link: four warps (directions) per 32 sites.
