@@ -24,21 +24,39 @@
 
 namespace ym {
 
+// Planes per thread of the plaquette-field kernel (below): two for the FP32
+// forms; one in FP64, where a pair needs 132 registers (2 blocks of 6 warps
+// per SM) and a single plane 80: at 32^4 on B200 the FP64 field kernel runs
+// 0.294 -> 0.270 ms per launch, the two-kernel FP64 step 1.80 -> 1.73 ms.
+template <class F>
+struct PlaqPlanesPerThread {
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 1 : 2;
+};
+
 // One thread per (site, pair of planes): six warps cover 64 sites, warps
 // 3k .. 3k + 2 the planes {(0,1), (0,2)}, {(0,3), (1,3)}, {(1,2), (2,3)} of
 // site group k (the two planes of a pair share one of the site's links,
 // loaded once).  The second plane's loads issue during the first plane's
 // products: against one plane per thread, the FP32-18 kernel ran 16 % faster
 // at 32^4 on B200 (0.180 -> 0.151 ms), the 12-real one 1.6 % (0.148 -> 0.146).
+// With one plane per thread (PlaqPlanesPerThread 1) six warps cover 32 sites,
+// warp w plane w.
 template <class F>
 __global__ void __launch_bounds__(192) plaq_field_kernel(F u, ForceField<typename F::Real> hf, Geo g) {
     const int w = int(threadIdx.x >> 5);
+    int c[4];
+    if (PlaqPlanesPerThread<F>::value == 1) {
+        const int s = g.site0 + int(blockIdx.x) * 32 + int(threadIdx.x & 31);
+        if (s >= g.site1) return;
+        g.coords(s, c);
+        hf.store(w, s, plane_generator(u, g, s, c, plane_a(w), plane_b(w)));
+        return;
+    }
     const int s = g.site0 + (int(blockIdx.x) * 2 + w / 3) * 32 + int(threadIdx.x & 31);
     if (s >= g.site1) return;
     const int pr = w % 3;
     const int p0 = pr == 0 ? 0 : (pr == 1 ? 2 : 3);
     const int p1 = pr == 0 ? 1 : (pr == 1 ? 4 : 5);
-    int c[4];
     g.coords(s, c);
     // both planes before either store: the link the two share is loaded once
     const auto h0 = plane_generator(u, g, s, c, plane_a(p0), plane_b(p0));
@@ -92,7 +110,8 @@ template <class F>
 static cudaError_t launch_plaq_typed(const void* u, void* h, const Geo& g, cudaStream_t st) {
     F in{const_cast<void*>(u), g.V};
     ForceField<typename F::Real> hf{h, g.V};
-    plaq_field_kernel<F><<<unsigned(((g.site1 - g.site0 + 31) / 32 + 1) / 2), 192, 0, st>>>(in, hf, g);
+    const unsigned groups = unsigned((g.site1 - g.site0 + 31) / 32);
+    plaq_field_kernel<F><<<PlaqPlanesPerThread<F>::value == 1 ? groups : (groups + 1) / 2, 192, 0, st>>>(in, hf, g);
     return cudaGetLastError();
 }
 
