@@ -207,10 +207,11 @@ YMFLOW_API int ymflow_time_kernels(ymflow_ctx* ctx, double eps, int nsteps, floa
  * (default), 0 = plain launches; YMFLOW_OPT_STAGE_FORM: the kernels of one RK3
  * stage (the reference's computeDerivative + exp + link update for all mu,
  * src/Apps/wilsonflow.cpp:143-171):
- *   0 = one fused kernel, staples summed per link (the FP64 default);
+ *   0 = one fused kernel, staples summed per link (the FP64 default where
+ *       form 1's field does not fit in device memory);
  *   1 = two kernels, the six plaquettes' generators of every site into a
  *       stored field (6 x 8 reals per site of device memory), then each link's
- *       force from them (the FP32 default);
+ *       force from them (the default);
  *   2 = one kernel: blocks of Lx x ty x tz sites of a time slice compute their
  *       plaquette generators into shared memory, recompute the lower (y, z)
  *       faces, stream along t and finish the links from there (whole-lattice

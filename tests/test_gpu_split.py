@@ -67,7 +67,7 @@ def test_fp32_split_meets_the_accuracy_target_at_t4(precision):
 def test_stage_form_defaults_and_refusals():
     from latticeyangmills_b200 import GluonField, YmflowError, _native as N
 
-    for prec, want in (("fp64", 0), ("fp32_18", 1), ("fp32_12", 1)):
+    for prec, want in (("fp64", 1), ("fp32_18", 1), ("fp32_12", 1)):
         with GluonField((4, 4, 4, 4), prec) as f:
             assert f.get_option(N.OPT_STAGE_FORM) == want
             with pytest.raises(YmflowError):

@@ -106,7 +106,7 @@ def test_tile_defaults_and_refusals():
         assert f.get_option(N.OPT_TILE) == tile_option(4, 4, 2, 1)  # the prepared default tiling
         f.set_option(N.OPT_STAGE_FORM, 2)
     with GluonField((32, 32, 32, 32), "fp64") as f:
-        assert f.get_option(N.OPT_STAGE_FORM) == 0
+        assert f.get_option(N.OPT_STAGE_FORM) == 1
         f.set_tile(2, 2)
         assert f.get_option(N.OPT_STAGE_FORM) == 2
         assert f.get_option(N.OPT_TILE) == tile_option(2, 2)
