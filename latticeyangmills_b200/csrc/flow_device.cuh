@@ -194,18 +194,20 @@ __device__ __forceinline__ Herm8<typename F::Real> plane_generator(const F& u, c
     const int s_pb = g.hop_rt(s, g.coord(c, b), b, +1);
     // lo = U_a(x) U_b(x+a) and up = U_b(x) U_a(x+b) (P = lo up^+), each
     // through its first two rows: rows 0 and 1 of the left link times the
-    // right link, row 2 = conj(row0 x row1) of the product, so the left
-    // link's row 2 is neither rebuilt nor multiplied.  36 of 162 multiply-adds
-    // per product fewer; the FP32-12 plaquette-field kernel at 32^4 on B200
-    // 0.150 -> 0.126 ms (with both planes of a pair formed before either is
-    // stored), |d(t^2 E)|/t^2 E against FP64 at t = 4 unchanged (1.0e-7).
-    M3<R> lo, up;
+    // right link; up's row 2 = conj(row0 x row1), and of P only rows 0 and 1
+    // are multiplied out (its row 2 from their cross product), so lo's row 2
+    // and the left links' rows 2 are never formed.  Against full-row
+    // products: 36 of 162 multiply-adds per product fewer, and 25 per plane
+    // in P; the FP32-12 plaquette-field kernel at 32^4 on B200 0.150 -> 0.126
+    // ms (two-row products, both planes of a pair formed before either is
+    // stored) -> 0.118 ms (P from its rows 0 and 1), |d(t^2 E)|/t^2 E
+    // against FP64 at t = 4 unchanged (1.0e-7).
+    Rows2<R> lo;
+    M3<R> up;
     {
-        Rows2<R> t;
         const Rows2<R> x = u.load_rows2(a, s);
         const M3<R> y = u.load(b, s_pa);
-        mmul_rows2<false, false>(x, y, t);
-        full_from_rows2(t, lo);
+        mmul_rows2<false, false>(x, y, lo);
     }
     {
         Rows2<R> t;
@@ -214,7 +216,7 @@ __device__ __forceinline__ Herm8<typename F::Real> plane_generator(const F& u, c
         mmul_rows2<false, false>(x, y, t);
         full_from_rows2(t, up);
     }
-    return force_from_b_cdag(lo, up);
+    return force_from_b2_cdag(lo, up);
 }
 
 // H_p(x) of plane p at site s into hf.

@@ -322,6 +322,47 @@ __device__ __forceinline__ Herm8<R> force_from_b_cdag(const M3<R>& b, const M3<R
     return z;
 }
 
+// The same generator of X = B C^+ for X in SU(3), from B's first two rows:
+// rows 0 and 1 of X (six entries), then of row 2 = conj(row0 x row1) only
+// X_20, X_21 and Im X_22.  92 multiply-adds, against 90 plus the 27 that
+// rebuild B's row 2 for the full form.
+template <class R>
+__device__ __forceinline__ Herm8<R> force_from_b2_cdag(const Rows2<R>& b, const M3<R>& c) {
+    Cx<R> x[2][3];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {  // (B C^+)_ij = sum_k b_ik conj(c_jk)
+            R re = R(0), im = R(0);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                re = fma(b.e[i][k].re, c.e[j][k].re, re);
+                re = fma(b.e[i][k].im, c.e[j][k].im, re);
+                im = fma(b.e[i][k].im, c.e[j][k].re, im);
+                im = fma(-b.e[i][k].re, c.e[j][k].im, im);
+            }
+            x[i][j] = cx(re, im);
+        }
+    // row 2 = conj(row0 x row1): X_2k = conj(X_0i X_1j - X_0j X_1i), (i, j) = (k+1, k+2) mod 3
+    auto cross = [&](int i, int j) {
+        const Cx<R> p = x[0][i], q = x[1][j], r = x[0][j], s = x[1][i];
+        const R re = fma(p.re, q.re, fma(-p.im, q.im, -fma(r.re, s.re, -r.im * s.im)));
+        const R im = fma(p.re, q.im, fma(p.im, q.re, -fma(r.re, s.im, r.im * s.re)));
+        return cx(re, -im);
+    };
+    const Cx<R> x20 = cross(1, 2), x21 = cross(2, 0);
+    const R i2 = -fma(x[0][0].re, x[1][1].im, fma(x[0][0].im, x[1][1].re, -fma(x[0][1].re, x[1][0].im, x[0][1].im * x[1][0].re)));
+    Herm8<R> z;
+    const R i0 = x[0][0].im, i1 = x[1][1].im;
+    const R mean = (i0 + i1 + i2) * R(1.0 / 3.0);
+    z.d0 = mean - i0;
+    z.d1 = mean - i1;
+    z.z01 = cx(R(-0.5) * (x[0][1].im + x[1][0].im), R(0.5) * (x[0][1].re - x[1][0].re));
+    z.z02 = cx(R(-0.5) * (x[0][2].im + x20.im), R(0.5) * (x[0][2].re - x20.re));
+    z.z12 = cx(R(-0.5) * (x[1][2].im + x21.im), R(0.5) * (x[1][2].re - x21.re));
+    return z;
+}
+
 // v^+ h v for a Hermitian traceless h: Hermitian and traceless again, so only
 // its diagonal d0, d1 and upper triangle are formed.  W = h v uses h's real
 // diagonal (h22 = -d0 - d1) and conjugate lower triangle.
