@@ -171,7 +171,7 @@ __device__ __forceinline__ int find_conf_param(const EnsTable& t, int item) {
 }
 
 template <class F>
-__global__ void __launch_bounds__(192) ens_plaq_param_kernel(char* u, char* h, const __grid_constant__ EnsTable tab) {
+__global__ void __launch_bounds__(192, PlaqMinBlocks<F>::value) ens_plaq_param_kernel(char* u, char* h, const __grid_constant__ EnsTable tab) {
     const int w = int(threadIdx.x >> 5);
     const int item = int(blockIdx.x) * 2 + w / 3;
     if (item >= tab.c[tab.n - 1].blk0 + tab.c[tab.n - 1].nblk) return;
@@ -251,7 +251,7 @@ struct EnsRun {
 };
 
 template <class F>
-__global__ void __launch_bounds__(192) ens_run_plaq_kernel(char* u, char* h, const __grid_constant__ EnsRun r) {
+__global__ void __launch_bounds__(192, PlaqMinBlocks<F>::value) ens_run_plaq_kernel(char* u, char* h, const __grid_constant__ EnsRun r) {
     const int w = int(threadIdx.x >> 5);
     const int item = int(blockIdx.x) * 2 + w / 3;
     const int conf = item / r.nblk;

@@ -41,8 +41,9 @@ struct PlaqPlanesPerThread {
 // at 32^4 on B200 (0.180 -> 0.151 ms), the 12-real one 1.6 % (0.148 -> 0.146).
 // With one plane per thread (PlaqPlanesPerThread 1) six warps cover 32 sites,
 // warp w plane w.
+
 template <class F>
-__global__ void __launch_bounds__(192) plaq_field_kernel(F u, ForceField<typename F::Real> hf, Geo g) {
+__global__ void __launch_bounds__(192, PlaqMinBlocks<F>::value) plaq_field_kernel(F u, ForceField<typename F::Real> hf, Geo g) {
     const int w = int(threadIdx.x >> 5);
     int c[4];
     if (PlaqPlanesPerThread<F>::value == 1) {
