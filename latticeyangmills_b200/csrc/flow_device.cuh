@@ -282,12 +282,15 @@ __device__ __forceinline__ void split_link_update(const F& in, const F& out, con
 // 32^4 on B200 against 1.05 at the 76 registers of 6 blocks; FP64 at 4 (its
 // fused kernel's budget).
 // Resident 192-thread blocks per SM the plaquette-field kernels are compiled
-// for: FP32 at 6 (56 registers, 36 warps per SM; 0.787 -> 0.764 ms per
-// FP32-12 step at 32^4 on B200 against the 64 registers of 5 blocks); FP64
-// unbounded (78 registers: at 5 or 6 blocks it spills, 1.73 -> 1.85 / 2.13 ms).
+// for: FP32 at 5 (64 registers, 30 warps per SM).  At 6 (56 registers, 8
+// bytes spilled) the FP32-12 step at 32^4 on B200 ran 3 % faster in short
+// bursts at full clock (0.787 -> 0.764 ms) but 1.5 % slower in the
+// power-capped steady state of a long flow (0.855 -> 0.868 ms, 2000-step
+// runs alternated on one GPU).  FP64 unbounded (78 registers: at 5 or 6
+// blocks it spills, 1.73 -> 1.85 / 2.13 ms).
 template <class F>
 struct PlaqMinBlocks {
-    static constexpr int value = sizeof(typename F::Real) == 8 ? 1 : 6;
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 1 : 5;
 };
 
 template <class F>
