@@ -154,7 +154,7 @@ def test_bench_byte_accounting_and_profiled_traffic():
     got = bench.profiled_traffic("fp32_12", (32, 32, 32, 32), alg, "rk_split_stage")
     assert got == pytest.approx(846300928 / 671088640 * alg)
     got = bench.profiled_traffic("fp32_12", (32, 32, 32, 32), alg, "plaq_field")
-    assert got == pytest.approx(369276672 / 402653184 * alg)
+    assert got == pytest.approx(369448704 / 402653184 * alg)
     got = bench.profiled_traffic("fp64", (32, 32, 32, 32), alg, "rk_stage")
     assert got == pytest.approx(1860280032 / 1744830464 * alg)
     assert bench.profiled_traffic("fp32_12", (16, 16, 16, 16), alg, "rk_split_stage") is None
