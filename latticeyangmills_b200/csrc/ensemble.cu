@@ -253,7 +253,10 @@ struct EnsRun {
 template <class F>
 __global__ void __launch_bounds__(192, PlaqMinBlocks<F>::value) ens_run_plaq_kernel(char* u, char* h, const __grid_constant__ EnsRun r) {
     const int w = int(threadIdx.x >> 5);
-    const int item = int(blockIdx.x) * 2 + w / 3;
+    // FP32: from the run's end, as plaq_field_kernel (its stage kernel starts
+    // on the L2-resident items)
+    const int blk = sizeof(typename F::Real) == 4 ? int(gridDim.x - 1 - blockIdx.x) : int(blockIdx.x);
+    const int item = blk * 2 + w / 3;
     const int conf = item / r.nblk;
     if (conf >= r.nconf) return;
     const Geo& g = r.g;
