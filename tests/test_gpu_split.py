@@ -157,3 +157,38 @@ def test_kernel_timing_splits_by_kernel():
         assert field / (3 * 4) < 0.01
         _, km = f.time_steps(0.01, 4, kernels=True)
         assert km > 0
+
+
+def test_fp64_context_without_room_for_the_plaquette_field_uses_the_fused_form():
+    """An FP64 context whose plaquette field (384 B per site) does not fit
+    beside its links starts in the fused form instead of failing, and flows as
+    a context with room does (to 1e-12)."""
+    import torch
+
+    from latticeyangmills_b200 import GluonField, YmflowError, _native as N
+
+    n = (32, 32, 32, 32)
+    sites = 32**4
+    need = 2 * 4 * sites * 144 + 4 * sites * 64  # both link buffers and the generator
+    field = 6 * sites * 64                        # the plaquette field
+
+    def run(f):
+        f.init_links("expiah", 0.35, 5)
+        return f.flow(0.02, 2, 1)
+
+    free, _ = torch.cuda.mem_get_info()
+    filler = torch.empty(int(free - need - field // 2), dtype=torch.uint8, device="cuda")
+    try:
+        with GluonField(n, "fp64") as f:
+            assert f.get_option(N.OPT_STAGE_FORM) == 0
+            with pytest.raises(YmflowError):
+                f.set_option(N.OPT_STAGE_FORM, 1)  # no room for the field either
+            got = run(f)
+    finally:
+        del filler
+        torch.cuda.empty_cache()
+    with GluonField(n, "fp64") as f:
+        assert f.get_option(N.OPT_STAGE_FORM) == 1
+        want = run(f)
+    np.testing.assert_array_equal(got[:, :2], want[:, :2])
+    np.testing.assert_allclose(got[:, [2, 4]], want[:, [2, 4]], rtol=1e-12)
