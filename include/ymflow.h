@@ -211,7 +211,8 @@ YMFLOW_API int ymflow_time_kernels(ymflow_ctx* ctx, double eps, int nsteps, floa
  *       form 1's field does not fit in device memory);
  *   1 = two kernels, the six plaquettes' generators of every site into a
  *       stored field (6 x 8 reals per site of device memory), then each link's
- *       force from them (the default);
+ *       force from them (the default, except FP32 lattices of at most 8192
+ *       sites, whose launch-bound steps run form 0);
  *   2 = one kernel: blocks of Lx x ty x tz sites of a time slice compute their
  *       plaquette generators into shared memory, recompute the lower (y, z)
  *       faces, stream along t and finish the links from there (whole-lattice

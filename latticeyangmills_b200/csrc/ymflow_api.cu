@@ -373,7 +373,9 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
     // stored plaquette field: at 32^4 on B200 0.77 against 1.16 ms per step
     // (FP32-12) and 1.73 against 2.05 (FP64).  Where the FP64 plaquette field
     // (384 bytes per site) does not fit beside the links, FP64 keeps the fused
-    // staple kernel.  The one-kernel form with a tile's plane generators in
+    // staple kernel.  FP32 lattices of at most 8192 sites, whose steps are
+    // bound by their launches, keep the one-launch fused kernel (8^4 FP32-12:
+    // 0.0164 against 0.0205 ms per step; from 12^4 on the two kernels win).  The one-kernel form with a tile's plane generators in
     // shared memory is prepared (its default tiling) for
     // YMFLOW_OPT_STAGE_FORM 2 and the autotuner, which times every form.
     if (r == YMFLOW_OK && prepare_tile_kernels(c->prec) != cudaSuccess) {
@@ -381,7 +383,8 @@ ymflow_ctx* ymflow_create(const int dims[4], int precision, int device, int* sta
         r = cuda_fail(c, e == cudaSuccess ? cudaErrorInvalidValue : e, "tile kernel set-up");
     }
     if (r == YMFLOW_OK) c->tile_ok = default_tile(c, &c->tile);
-    if (r == YMFLOW_OK) {
+    const bool launch_bound = c->prec != YMFLOW_FP64 && V <= 8192;
+    if (r == YMFLOW_OK && !launch_bound) {
         r = dev_alloc(c, &c->hfield, plane_field_bytes(c->prec, V), "plaquette field");
         if (r == YMFLOW_OK) {
             c->stage_form = 1;

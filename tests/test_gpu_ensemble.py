@@ -9,11 +9,12 @@ SIZES = [(4, 4, 4, 4), (3, 4, 5, 6), (2, 3, 2, 4), (6, 6, 6, 8), (8, 8, 8, 8)]
 
 
 def single(n, prec, seed, steps, every):
-    # single contexts and the ensemble run the same stage form (fused in FP64,
-    # the two-kernel stage in FP32)
-    from latticeyangmills_b200 import GluonField
+    # the single contexts run the ensemble's stage form (fused in FP64, the
+    # two-kernel stage in FP32)
+    from latticeyangmills_b200 import GluonField, _native as N
 
     with GluonField(n, prec) as f:
+        f.set_option(N.OPT_STAGE_FORM, 0 if prec == "fp64" else 1)
         f.init_links("expiah", 0.3 + 0.02 * seed, seed)
         rows = f.flow(0.01, steps, every)
         return rows, f.download()

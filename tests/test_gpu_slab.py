@@ -11,8 +11,9 @@ N8 = (8, 4, 4, 10)  # spatial volume 128 (whole warp groups), 10 time slices
 
 
 def whole(precision, n=N8, seed=11, steps=6, every=2):
-    # slabs and the whole lattice run the same stage form (fused in FP64, the
-    # two-kernel stage in FP32)
+    # slabs and the whole lattice run the same stage form (the default for
+    # their sizes: the fused kernel for these small FP32 lattices, the
+    # two-kernel stage in FP64)
     from latticeyangmills_b200 import GluonField
 
     with GluonField(n, precision) as f:

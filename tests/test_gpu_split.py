@@ -67,12 +67,16 @@ def test_fp32_split_meets_the_accuracy_target_at_t4(precision):
 def test_stage_form_defaults_and_refusals():
     from latticeyangmills_b200 import GluonField, YmflowError, _native as N
 
-    for prec, want in (("fp64", 1), ("fp32_18", 1), ("fp32_12", 1)):
-        with GluonField((4, 4, 4, 4), prec) as f:
+    # the two-kernel form, except FP32 lattices of at most 8192 sites (launch-bound: the fused kernel)
+    for n, prec, want in (((4, 4, 4, 4), "fp64", 1), ((4, 4, 4, 4), "fp32_18", 0), ((8, 8, 8, 8), "fp32_12", 0),
+                          ((8, 8, 8, 18), "fp32_12", 1), ((8, 8, 8, 16), "fp32_18", 0)):
+        with GluonField(n, prec) as f:
             assert f.get_option(N.OPT_STAGE_FORM) == want
             with pytest.raises(YmflowError):
                 f.set_option(N.OPT_STAGE_FORM, 2)
-    with GluonField.slab((8, 4, 4, 10), 0, 5, "fp32_18") as s:
+            f.set_option(N.OPT_STAGE_FORM, 1)  # the plaquette field is allocated on demand
+            assert f.get_option(N.OPT_STAGE_FORM) == 1
+    with GluonField.slab((32, 8, 8, 10), 0, 5, "fp32_18") as s:  # 32 x 8 x 8 x 7 local sites
         assert s.get_option(N.OPT_STAGE_FORM) == 1
         s.set_option(N.OPT_STAGE_FORM, 0)
         assert s.get_option(N.OPT_STAGE_FORM) == 0
@@ -86,6 +90,7 @@ def test_slab_group_needs_one_stage_form():
     try:
         for sl in (a, b):
             sl.init_links("expiah", 0.4, 3)
+        a.set_option(N.OPT_STAGE_FORM, 1)
         b.set_option(N.OPT_STAGE_FORM, 0)
         with pytest.raises(YmflowError):
             slab_group_flow([a, b], 0.02, 2, 1)
