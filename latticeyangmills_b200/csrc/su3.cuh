@@ -213,10 +213,13 @@ __device__ __forceinline__ void full_from_rows2(const Rows2<R>& a, M3<R>& m) {
 
 // Products of SU(3) links through their first two rows (third row rebuilt as conj(r0 x r1))
 // save 22% of the staple multiply-adds but rebuild a row from rounded rows.
-// In FP64 that costs nothing measurable; in FP32 the rebuilt rows carry a
-// systematic bias that grows linearly with flow time (t^2<E> at t = 4 on 32^4
-// drifts 4e-6 from FP64 against 5e-7 with full products), so the FP32 path
-// forms all three rows.
+// In FP64 that costs nothing measurable; in FP32 the rebuilt rows of the fused
+// kernel's staples carried a systematic bias that grew linearly with flow time
+// (t^2<E> at t = 4 on 32^4 drifted 4e-6 from FP64 against 5e-7 with full
+// products, measured before the link update took its e^{iQ} - 1 form), so the
+// fused kernel's FP32 staples form all three rows.  The plaquette field and
+// the observables form their products through two rows in every precision
+// (t = 4 error against FP64 1.0e-7 either way).
 template <class R>
 struct kTwoRowStaples {
     static constexpr bool value = sizeof(R) == 8;
