@@ -1,8 +1,11 @@
 // K6: batched ensemble.  Many configurations of uneven lattice sizes advance
-// through each RK3 stage in ONE persistent launch: the work list is every
-// (configuration, block of sites) pair, a fixed grid of CTAs walks it with a
-// grid-stride loop, and each item looks its configuration up in a prefix table.
-// The three stage launches of a step are replayed as a captured CUDA graph.
+// through each RK3 stage together: in one launch per kernel over a work list
+// of every (configuration, block of sites) pair, each item looking its
+// configuration up in a prefix table (the per-link kernel over a persistent
+// grid-stride loop or one block per item, the two-kernel stage, the tile
+// kernel), or in two launches per run of equal-extent configurations, the
+// runs as concurrent branches (stage form 3).  The launches of a step are
+// replayed as a captured CUDA graph; the project's autotuner picks the form.
 // The reference flows its configurations one after another
 // (src/Apps/wilsonflow.cpp:96-109); small lattices cannot fill a B200 that way.
 #include <cuda_runtime.h>
