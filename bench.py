@@ -7,7 +7,7 @@ every 10th step inside the timed region (the 32^4 configuration's schedule).
 The stage form (fused kernel, two kernels through a stored plaquette field,
 or one kernel with a tile's plaquette field in shared memory) is the
 project's autotuner's choice for the lattice and precision; on B200 it picks
-the two-kernel stage for FP32 and the fused kernel for FP64.  The default
+the two-kernel stage at 32^4 in every precision.  The default
 precision is the 12-real FP32 form.  Inputs are seeded
 synthetic fields U = e^{i a H} (a = 0.35, H Gaussian traceless Hermitian per
 link), generated on the device; 32^4 links plus the generator field are larger
