@@ -388,9 +388,10 @@ YMFLOW_API int ymflow_ensemble_time_steps(ymflow_ens* ens, double eps, int nstep
  *   - the per-link kernel (FP64) over persistent grids {one CTA per work
  *     item, 1x and 2x the resident CTAs}, or the two-kernel stage (FP32), one
  *     block per 32-site item;
- *   - (FP32) the two-kernel stage launched once per run of consecutive
+ *   - the two-kernel stage launched once per run of consecutive
  *     configurations with equal extents, each run's geometry a launch
- *     parameter (two launches per run and stage);
+ *     parameter (two launches per run and stage; FP64 ensembles where their
+ *     plane-generator pool fits);
  *   - the one-kernel stage with tiles in shared memory (YMFLOW_OPT_STAGE_FORM
  *     2 of a single context) at 128, 256, 384 or 512 threads per block: every
  *     configuration gets the tile of at most that many sites (whole x lines,
@@ -405,8 +406,9 @@ YMFLOW_API int ymflow_ensemble_autotune(ymflow_ens* ens, double eps, int* block,
  * block size and grid. */
 YMFLOW_API int ymflow_ensemble_tuning(const ymflow_ens* ens, int* stage_form, int* block, int* grid);
 /* Sets the form by hand: 0 with block 128 and a grid (0: one block per item),
- * 1 or 3 (FP32 ensembles) with block 128, or 2 with `block` threads (grid
- * chosen from the occupancy).  YMFLOW_ERR_ARG where the form cannot run. */
+ * 1 or 3 with block 128 (ensembles with a plane-generator pool: every FP32
+ * one, FP64 ones where it fits), or 2 with `block` threads (grid chosen from
+ * the occupancy).  YMFLOW_ERR_ARG where the form cannot run. */
 YMFLOW_API int ymflow_ensemble_set_tuning(ymflow_ens* ens, int stage_form, int block, int grid);
 
 #ifdef __cplusplus

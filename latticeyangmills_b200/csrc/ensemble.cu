@@ -256,9 +256,23 @@ struct EnsRun {
 template <class F>
 __global__ void __launch_bounds__(192, PlaqMinBlocks<F>::value) ens_run_plaq_kernel(char* u, char* h, const __grid_constant__ EnsRun r) {
     const int w = int(threadIdx.x >> 5);
+    if constexpr (sizeof(typename F::Real) == 8) {  // FP64: one plane per thread, warp w plane w of one item
+        const int item = int(blockIdx.x);
+        const int conf = item / r.nblk;
+        if (conf >= r.nconf) return;
+        const Geo& g = r.g;
+        const int s = (item - conf * r.nblk) * 32 + int(threadIdx.x & 31);
+        if (s >= g.V) return;
+        const F uf{u + conf * r.ustride, g.V};
+        const ForceField<typename F::Real> hf{h + conf * r.hstride, g.V};
+        int c[4];
+        g.coords(s, c);
+        hf.store(w, s, plane_generator(uf, g, s, c, plane_a(w), plane_b(w)));
+        return;
+    }
     // FP32: from the run's end, as plaq_field_kernel (its stage kernel starts
     // on the L2-resident items)
-    const int blk = sizeof(typename F::Real) == 4 ? int(gridDim.x - 1 - blockIdx.x) : int(blockIdx.x);
+    const int blk = int(gridDim.x - 1 - blockIdx.x);
     const int item = blk * 2 + w / 3;
     const int conf = item / r.nblk;
     if (conf >= r.nconf) return;
@@ -309,7 +323,7 @@ static cudaError_t launch_ens_run_typed(int stage, void* uin, void* uout, void* 
     const R e = R(stage == 0 ? eps * 0.25 : eps);
     const int items = L.r.nconf * L.r.nblk;
     char *a = (char*)uin + L.uoff, *b = (char*)uout + L.uoff, *zz = (char*)z + L.zoff, *hh = (char*)h + L.hoff;
-    ens_run_plaq_kernel<F><<<(items + 1) / 2, 192, 0, st>>>(a, hh, L.r);
+    ens_run_plaq_kernel<F><<<sizeof(R) == 8 ? items : (items + 1) / 2, 192, 0, st>>>(a, hh, L.r);
     switch (stage) {
         case 0: ens_run_split_kernel<F, 0><<<items, 128, 0, st>>>(a, b, zz, hh, L.r, e); break;
         case 1: ens_run_split_kernel<F, 1><<<items, 128, 0, st>>>(a, b, zz, hh, L.r, e); break;
@@ -321,6 +335,7 @@ static cudaError_t launch_ens_run_typed(int stage, void* uin, void* uout, void* 
 cudaError_t launch_ens_run_stage(int prec, int stage, void* uin, void* uout, void* z, void* h, const EnsRunLaunch& L,
                                  double eps, cudaStream_t st) {
     switch (prec) {
+        case kFP64: return launch_ens_run_typed<FieldD18>(stage, uin, uout, z, h, L, eps, st);
         case kFP32_18: return launch_ens_run_typed<FieldF18>(stage, uin, uout, z, h, L, eps, st);
         case kFP32_12: return launch_ens_run_typed<FieldF12>(stage, uin, uout, z, h, L, eps, st);
         default: return cudaErrorInvalidValue;
@@ -626,6 +641,8 @@ int nitems(const ymflow_ens* e) {
 // back to one 128-thread block per work item.
 int apply_tuning(ymflow_ens* e, const EnsTuning& tn) {
     e->by_runs = tn.form == 3;
+    if (tn.form == 0) e->split = false;
+    if (tn.form == 1 || tn.form == 3) e->split = true;
     if (tn.form == 2 && set_tiles(e, tn.block)) {
         e->tile = true;
         return YMFLOW_OK;
@@ -860,8 +877,18 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
     if (r == YMFLOW_OK) r = ens_alloc(e, &e->u[1], size_t(uo), "link pool 1");
     if (r == YMFLOW_OK) r = ens_alloc(e, &e->z, size_t(zo), "generator pool");
     // FP32 ensembles flow with the two-kernel stage, as FP32 single contexts do
+    // FP32 ensembles flow with the two-kernel stage, FP64 ones with the fused
+    // kernel until the autotuner or ymflow_ensemble_set_tuning picks the
+    // per-run two-kernel form; an FP64 ensemble without room for the plane
+    // generators keeps the fused kernel only
     e->split = precision != YMFLOW_FP64;
-    if (r == YMFLOW_OK && e->split) r = ens_alloc(e, &e->h, size_t(ho), "plane-generator pool");
+    if (r == YMFLOW_OK) {
+        r = ens_alloc(e, &e->h, size_t(ho), "plane-generator pool");
+        if (r == YMFLOW_ERR_OOM && !e->split) {
+            r = YMFLOW_OK;
+            e->err.clear();
+        }
+    }
     for (int c = 0; c < nconf; c++) {  // runs of consecutive configurations with equal extents
         const EnsConf& C = e->confs[c];
         if (c > 0 && std::equal(C.g.n, C.g.n + 4, e->confs[c - 1].g.n)) {
@@ -880,7 +907,7 @@ ymflow_ens* ymflow_ensemble_create(int nconf, const int* dims, int precision, in
         L.hoff = C.hoff;
         e->runs.push_back(L);
     }
-    if (r == YMFLOW_OK && e->split && e->runs.size() > 1) {  // up to four concurrent branches
+    if (r == YMFLOW_OK && e->h && e->runs.size() > 1) {  // up to four concurrent branches
         const size_t ns = std::min<size_t>(e->runs.size(), 4);
         if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) r = YMFLOW_ERR_CUDA;
         for (size_t k = 0; k < ns && r == YMFLOW_OK; k++) {
@@ -1126,12 +1153,13 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     // resident blocks} (FP64) or the two-kernel stage (FP32), and the tile
     // kernel with 128 / 256 / 384 / 512 threads (tiles of at most that many sites)
     std::vector<EnsTuning> cands;
-    if (e->split) {
+    if (e->prec != YMFLOW_FP64) {
         cands.push_back({1, 128, 0});
         cands.push_back({3, 128, 0});
     } else {
         const int resident = ens_max_resident(e->prec, 128);
         for (int grid : {0, resident * sms, 2 * resident * sms}) cands.push_back({0, 128, grid});
+        if (e->h) cands.push_back({3, 128, 0});
     }
     for (int threads : {128, 256, 384, 512}) cands.push_back({2, threads, 0});
     const bool was_split = e->split;
@@ -1140,6 +1168,7 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
     for (const EnsTuning& ch : cands) {
         e->tile = false;
         e->by_runs = ch.form == 3;
+        e->split = ch.form == 1 || ch.form == 3;
         if (ch.form == 2) {
             if (!set_tiles(e, ch.block)) continue;
             e->tile = true;
@@ -1155,7 +1184,7 @@ int ymflow_ensemble_autotune(ymflow_ens* e, double eps, int* block_out, int* gri
             pick = ch;
         }
     }
-    e->split = was_split;
+    e->split = was_split;  // a tile pick flows over the form the ensemble had
     const int r = apply_tuning(e, pick);
     if (r != YMFLOW_OK) return r;
     drop_graphs(e);
@@ -1188,7 +1217,7 @@ int ymflow_ensemble_set_tuning(ymflow_ens* e, int stage_form, int block, int gri
         const int r = set_block(e, 128);
         if (r != YMFLOW_OK) return r;
     } else {
-        return efail(e, YMFLOW_ERR_ARG, "stage form is 0, 1 or 3 (FP32 ensembles) or 2");
+        return efail(e, YMFLOW_ERR_ARG, "stage form is 0, 1, 2 or 3 (1 and 3 need the plane-generator pool)");
     }
     YE_CK(e, cudaStreamSynchronize(e->stream), "set tuning");
     drop_graphs(e);

@@ -286,11 +286,13 @@ __device__ __forceinline__ void split_link_update(const F& in, const F& out, con
 // bytes spilled) the FP32-12 step at 32^4 on B200 ran 3 % faster in short
 // bursts at full clock (0.787 -> 0.764 ms) but 1.5 % slower in the
 // power-capped steady state of a long flow (0.855 -> 0.868 ms, 2000-step
-// runs alternated on one GPU).  FP64 unbounded (78 registers: at 5 or 6
-// blocks it spills, 1.73 -> 1.85 / 2.13 ms).
+// runs alternated on one GPU).  FP64 at 4 (80 registers, one plane per
+// thread: 0.274 -> 0.266 ms per launch at 32^4 against the 146 registers the
+// compiler takes unbounded; at 5 or 6 blocks it spills and the step goes
+// 1.73 -> 1.85 / 2.13 ms).
 template <class F>
 struct PlaqMinBlocks {
-    static constexpr int value = sizeof(typename F::Real) == 8 ? 1 : 5;
+    static constexpr int value = sizeof(typename F::Real) == 8 ? 4 : 5;
 };
 
 template <class F>

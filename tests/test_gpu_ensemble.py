@@ -116,7 +116,9 @@ def test_set_tuning_refusals():
         assert ens.tuning()[0] == 1
     with Ensemble([(8, 8, 8, 8)], "fp64") as ens:
         with pytest.raises(YmflowError):
-            ens.set_tuning(1)  # no plane-generator pool in FP64 ensembles
+            ens.set_tuning(4)  # no such form
+        with pytest.raises(YmflowError):
+            ens.set_tuning(3, 256)  # the two-kernel stage runs 128 threads
 
 
 # runs of equal extents: two of 8^4, one of 3x4x5x6, three of 6^3x8, one of 8^4
@@ -143,8 +145,25 @@ def test_per_run_two_kernel_stage_equals_work_list_form(prec):
     np.testing.assert_array_equal(out[3][0], out[1][0])
     for a, b in zip(out[3][1], out[1][1]):
         np.testing.assert_array_equal(a, b)
-    with Ensemble([(8, 8, 8, 8)], "fp64") as ens:
-        from latticeyangmills_b200 import YmflowError
 
-        with pytest.raises(YmflowError):
-            ens.set_tuning(3)  # FP64 ensembles have no plane-generator pool
+
+def test_fp64_per_run_two_kernel_stage_equals_the_fused_form():
+    """FP64 ensembles flow with the fused kernel by default; the per-run
+    two-kernel form (stage form 3) gives the same flow to FP64 rounding, and
+    the reference's golden rows to 1e-12."""
+    from latticeyangmills_b200 import Ensemble
+
+    out = {}
+    for form in (0, 3):
+        with Ensemble(RUN_SIZES, "fp64") as ens:
+            assert ens.tuning()[0] == 0
+            ens.set_tuning(form)
+            assert ens.tuning()[0] == form
+            for c in range(len(RUN_SIZES)):
+                ens.init_links(c, "expiah", 0.3 + 0.02 * c, 20 + c)
+            rows = ens.flow(0.02, 6, 3)
+            out[form] = (rows, [ens.download(c) for c in range(len(RUN_SIZES))])
+    np.testing.assert_array_equal(out[3][0][:, :, :2], out[0][0][:, :, :2])
+    np.testing.assert_allclose(out[3][0][:, :, [2, 4]], out[0][0][:, :, [2, 4]], rtol=1e-12)
+    for a, b in zip(out[3][1], out[0][1]):
+        assert np.abs(a - b).max() < 1e-13
