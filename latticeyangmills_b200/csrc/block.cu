@@ -286,18 +286,19 @@ int ymflow_block_group_flow(ymflow_ctx* const* ctxs, int n, const int grid[4], d
                 DeviceGuard g(c->device);
                 YM_CK(c, enqueue_stage(c, stage, c->u[c->cur], c->u[1 - c->cur], eps), "stage launch");
                 c->cur = 1 - c->cur;
+                // The reunitarisation goes before the step's last exchange:
+                // the neighbours then pull the reunitarised links into their
+                // halos.  After the exchange it would rewrite links that a
+                // neighbour's pull may still be reading.
+                if (stage == 2 && reunit && s % reunit_every == 0)
+                    YM_CK(c, launch_reunitarize(c->prec, c->u[c->cur], c->geo, c->deviation, c->stream),
+                          "reunitarise");
             }
             if ((r = block_exchange(ctxs, n, G, evs.ev)) != YMFLOW_OK) return r;
         }
         for (int i = 0; i < n; i++) {
-            ymflow_ctx* c = ctxs[i];
-            c->step++;
-            c->t += eps;
-            if (reunit && s % reunit_every == 0) {
-                // every local site, halos included: the same links as their owners'
-                DeviceGuard g(c->device);
-                YM_CK(c, launch_reunitarize(c->prec, c->u[c->cur], c->geo, c->deviation, c->stream), "reunitarise");
-            }
+            ctxs[i]->step++;
+            ctxs[i]->t += eps;
         }
         if ((measure_every > 0 && s % measure_every == 0) || s == nsteps) {
             if ((r = measure(row)) != YMFLOW_OK) return r;

@@ -376,6 +376,12 @@ int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nstep
                               "stage launch");
                     }
                     c->cur = 1 - c->cur;
+                    // before the step's last exchange, whose copies then carry
+                    // the reunitarised links (after it, the reunitarisation
+                    // would rewrite links a neighbour's copy may still read)
+                    if (stage == 2 && reunit && s % reunit_every == 0)
+                        YM_CK(c, launch_reunitarize(c->prec, c->u[c->cur], c->geo, c->deviation, c->stream),
+                              "reunitarise");
                 }
                 if ((r = exchange_current()) != YMFLOW_OK) return r;
             }
@@ -385,7 +391,9 @@ int ymflow_slab_group_flow(ymflow_ctx* const* ctxs, int n, double eps, int nstep
             // three stages flipped the buffer three times; the step's result is the third stage's
             c->step++;
             c->t += eps;
-            if (reunit && s % reunit_every == 0) {
+            if (fused && reunit && s % reunit_every == 0) {
+                // every local site, halos included (the neighbours' stages stored
+                // them before group_order): the same links as their owners'
                 DeviceGuard g(c->device);
                 YM_CK(c, launch_reunitarize(c->prec, c->u[c->cur], c->geo, c->deviation, c->stream), "reunitarise");
             }
